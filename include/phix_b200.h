@@ -1,0 +1,179 @@
+/*
+ * phix_b200.h -- C ABI of the B200-native PhiX time-step library
+ * (libphix_b200.so, built from phix_b200/csrc for sm_100a).
+ *
+ * Every entry point takes plain device pointers, sizes and POD descriptors,
+ * never throws, and returns PHIX_OK (0) or a negative status; the message of
+ * the last failure on the calling thread is available from phix_last_error().
+ * The C++ drop-in API (include/phix/...) turns a negative status into the
+ * exception type the reference throws (std::runtime_error for CUDA failures,
+ * std::invalid_argument for shape and argument errors).
+ *
+ * Field layout.  A field is the reference's ghost-padded stored array
+ * (ScalarField.h:15-27): stored dims n[a] + 2*ghost on every axis, unused
+ * axes of 1-D/2-D meshes included, x fastest, FP64.  Kernels write physical
+ * cells; ghost cells are only ever filled the way the reference fills them.
+ *
+ * Streams.  `stream` arguments are cudaStream_t values passed as void*;
+ * NULL means the legacy default stream.  Calls are asynchronous unless the
+ * name says otherwise.
+ */
+#ifndef PHIX_B200_H
+#define PHIX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHIX_ABI_VERSION 1
+
+/* status codes */
+#define PHIX_OK 0
+#define PHIX_ERR_ARG (-1)         /* bad argument / shape (std::invalid_argument) */
+#define PHIX_ERR_CUDA (-2)        /* CUDA runtime failure (std::runtime_error)     */
+#define PHIX_ERR_UNSUPPORTED (-3) /* combination not built                        */
+#define PHIX_ERR_NONFINITE (-4)   /* diagnostics found NaN/Inf in a field         */
+
+/* boundary condition kinds, per axis side (Boundary.cu:95-195) */
+#define PHIX_BC_NONE 0     /* ghost cells left as stored                    */
+#define PHIX_BC_PERIODIC 1 /* PeriodicBC: ghost <- opposite physical layer  */
+#define PHIX_BC_NOFLUX 2   /* NoFluxBC: ghost <- nearest physical cell      */
+#define PHIX_BC_FIXED 3    /* FixedBC: ghost <- constant bc_val             */
+
+/* built-in physics (right-hand sides of the reference's drivers) */
+#define PHIX_PHYS_AC 0   /* prm = [L, kappa]:  L*kappa*lap(phi) + L*pw(phi, p - p^3)          */
+#define PHIX_PHYS_CH 1   /* prm = [M, kappa, rho, ca, cb]:  M*lap(f'(c) - kappa*lap(c), bcs),
+                            f'(c) = 2 rho (c-ca)(c-cb)(2c-ca-cb)                               */
+#define PHIX_PHYS_CHAC 2 /* prm = [M, L, kappa_c, kappa_eta, lambda]; fields (c, eta):
+                            c  : M*lap(f_c(c,eta) - kappa_c*lap(c), bcs)
+                            eta: (-L)*f_eta(eta,c) + (L*kappa_eta)*lap(eta)
+                            f = c^2(1-c)^2 + eta^2(1-eta)^2 + lambda c^2 eta^2                 */
+
+/* time schemes (Solver.h:17-20) */
+#define PHIX_EULER 0
+#define PHIX_RK4 1
+
+/* arithmetic of the stencil kernels */
+#define PHIX_F64 0
+#define PHIX_F32 1
+
+/* Mesh + boundary description.  n[a] = 1 and d[a] = 1 for unused axes. */
+typedef struct {
+    int32_t dim;        /* 1, 2 or 3                                   */
+    int32_t n[3];       /* physical cells per axis                     */
+    int32_t ghost;      /* ghost layers of the stored layout (>= 1)    */
+    int32_t bc_type[6]; /* [2*axis + side], side 0 = low, 1 = high     */
+    int32_t reserved;   /* must be 0                                   */
+    double d[3];        /* spacing                                     */
+    double bc_val[6];   /* value for PHIX_BC_FIXED sides               */
+} phix_grid_t;
+
+typedef struct phix_stepper phix_stepper_t;
+
+/* ---- library ---------------------------------------------------------- */
+int phix_abi_version(void);
+const char* phix_last_error(void);
+/* Number of kernel launches this library has issued in this process. */
+long long phix_launch_count(void);
+
+/* ---- single operators (replace the reference's per-term kernels) ------- */
+
+/* Ghost refresh with every BC of `g`, in buildBCs order.
+ * Replaces PeriodicBC/NoFluxBC/FixedBC::applyOnGPU (Boundary.cu:224-351). */
+int phix_bc_apply(double* field, const phix_grid_t* g, void* stream);
+
+/* rhs += coeff * lap(src) on physical cells.
+ * Replaces kernel_lap_accumulate + lap(f) (Equation.cu:40-80, :130-183). */
+int phix_lap_accumulate(double* rhs, const double* src, double coeff, const phix_grid_t* g, void* stream);
+
+/* rhs += coeff * d(src)/dx_axis, central difference.
+ * Replaces kernel_grad_accumulate + grad(f, axis) (Equation.cu:89-124, :185-240). */
+int phix_grad_accumulate(double* rhs, const double* src, double coeff, int axis, const phix_grid_t* g,
+                         void* stream);
+
+/* Built-in pointwise functors for phix_pointwise_accumulate. */
+#define PHIX_PW_IDENT 0  /* f(a)    = a                                   */
+#define PHIX_PW_AC 1     /* f(a)    = a - a^3   (tutorials/quickstart)    */
+#define PHIX_PW_DW 2     /* f(a)    = 2 rho (a-ca)(a-cb)(2a-ca-cb), prm = physics CH prm */
+#define PHIX_PW_CHAC_C 3 /* f(c,e)  = f_c of PHIX_PHYS_CHAC, prm[4] = lambda              */
+#define PHIX_PW_CHAC_E 4 /* f(e,c)  = f_eta of PHIX_PHYS_CHAC, prm[4] = lambda            */
+#define PHIX_PW_MUL 5    /* f(a,b)  = a*b                                 */
+
+/* rhs += coeff * f(s1[, s2]) on physical cells.
+ * Replaces kernel_pw_accumulate / kernel_pw2_accumulate (TermPW.inl:18-63)
+ * for the functors above (user functors are instantiated by the C++ API). */
+int phix_pointwise_accumulate(double* rhs, const double* s1, const double* s2, double coeff, int func,
+                              const double* prm, const phix_grid_t* g, void* stream);
+
+/* rhs += coeff * s1 * s2 on physical cells.
+ * Replaces kernel_mul_accumulate (Equation.cu:386-404). */
+int phix_mul_accumulate(double* rhs, const double* s1, const double* s2, double coeff, const phix_grid_t* g,
+                        void* stream);
+
+/* dst[i] += coeff * src[i] over n stored elements.
+ * Replaces kernel_axpy (Solver.cu:30-35). */
+int phix_axpy(double* dst, const double* src, double coeff, size_t n, void* stream);
+
+/* ---- fused time stepper (Solver / VectorSolver replacement) ------------ */
+
+/* Create a stepper for one built-in physics.  It owns the stage buffers
+ * (RK4: k1..k3 per field), a second state buffer per field, an internal
+ * stream and any captured CUDA graphs.  precision = PHIX_F64 works on the
+ * reference layout in FP64; PHIX_F32 keeps an FP32 copy of the state and
+ * runs the stencil arithmetic in FP32.
+ * Replaces Solver(Equation&, bcs, dt, scheme) (Solver.cu:86-107) and
+ * VectorSolver (VectorSolver.cu:77-100). */
+int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precision, const double* prm, double dt,
+                        const phix_grid_t* g);
+int phix_stepper_destroy(phix_stepper_t* h);
+int phix_stepper_nfields(const phix_stepper_t* h);
+
+/* Copy the state in from / out to FP64 stored device arrays (one per field),
+ * converting precision when the stepper is FP32.  Ordered on `stream`. */
+int phix_stepper_load(phix_stepper_t* h, const double* const* fields, void* stream);
+int phix_stepper_store(phix_stepper_t* h, double* const* fields, void* stream);
+
+/* Advance nsteps time steps on `stream`.  Each step is one launch per RK
+ * stage (4 for RK4, 1 for Euler) with the BCs, the stage combination and the
+ * final update fused in.  When steps_per_graph > 0 (see
+ * phix_stepper_set_graph) whole groups of steps replay as one CUDA graph.
+ * Replaces Solver::advance / VectorSolver::advance (Solver.cu:366-382). */
+int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream);
+
+/* Replay groups of `steps_per_graph` steps from a captured CUDA graph
+ * (0 disables graphs).  Replaces the driver step loop (Solver::run,
+ * Solver.cu:405-414) between callbacks. */
+int phix_stepper_set_graph(phix_stepper_t* h, int steps_per_graph);
+
+/* FP64 only: run directly on caller-owned buffers, no copies.  fields[f] is
+ * the current state and alt[f] a second stored array of the same size.
+ * After phix_stepper_advance, phix_stepper_current() reports which of the two
+ * holds the newest state (0: fields, 1: alt); the drop-in Solver swaps
+ * ScalarField::d_curr / d_prev accordingly. */
+int phix_stepper_bind(phix_stepper_t* h, double* const* fields, double* const* alt);
+int phix_stepper_current(const phix_stepper_t* h);
+
+/* End-to-end convenience: host FP64 stored arrays in, nsteps, host arrays
+ * out (host->device copy, advance, device->host copy, synchronise). */
+int phix_stepper_run_host(phix_stepper_t* h, const double* const* host_in, double* const* host_out, int nsteps);
+
+/* ---- diagnostics (FP64 accumulation) ----------------------------------- */
+
+/* out[0] = sum_phys u * dV (mass), out[1] = free energy
+ *   sum_phys [ f(u) + kappa/2 |grad u|^2 ] * dV
+ * with the physics' bulk energy density and central gradients on BC-mapped
+ * neighbours (develop/Spinodal Decomposition/computeFreeEnergy.py:76-98).
+ * fields: 1 (AC, CH) or 2 (CHAC) FP64 stored device arrays.  Synchronous.
+ * Returns PHIX_ERR_NONFINITE if any physical value is NaN/Inf. */
+int phix_reduce_mass_energy(const double* const* fields, int phys, const double* prm, const phix_grid_t* g,
+                            double* out, void* stream);
+/* Same diagnostics on the stepper's own current state (FP32 or FP64). */
+int phix_stepper_diagnostics(phix_stepper_t* h, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHIX_B200_H */

@@ -1,0 +1,262 @@
+"""phix_b200 -- B200-native (sm_100a) PhiX finite-difference time step.
+
+This module is the ctypes binding of the C ABI in include/phix_b200.h
+(libphix_b200.so, built in-tree by phix_b200/build.py).  It is what a Python
+caller of the library binds; the C++ drop-in API lives in include/phix/.
+Device memory and streams come from PyTorch (plumbing only); every kernel is
+the library's own.  There is no CPU fallback: without the shared library or a
+GPU every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libphix_b200.so")
+
+OK, ERR_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2, -3, -4
+BC_NONE, BC_PERIODIC, BC_NOFLUX, BC_FIXED = 0, 1, 2, 3
+PHYS_AC, PHYS_CH, PHYS_CHAC = 0, 1, 2
+EULER, RK4 = 0, 1
+F64, F32 = 0, 1
+PW_IDENT, PW_AC, PW_DW, PW_CHAC_C, PW_CHAC_E, PW_MUL = range(6)
+
+NFIELDS = {PHYS_AC: 1, PHYS_CH: 1, PHYS_CHAC: 2}
+
+
+class PhixError(RuntimeError):
+    """Status < 0 from the library.  `code` is the PHIX_ERR_* value."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class PhixArgumentError(PhixError, ValueError):
+    """PHIX_ERR_ARG: the analogue of the reference's std::invalid_argument."""
+
+
+class GridT(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32),
+        ("n", C.c_int32 * 3),
+        ("ghost", C.c_int32),
+        ("bc_type", C.c_int32 * 6),
+        ("reserved", C.c_int32),
+        ("d", C.c_double * 3),
+        ("bc_val", C.c_double * 6),
+    ]
+
+
+def make_grid(n: Sequence[int], d: Sequence[float] = (1.0, 1.0, 1.0), ghost: int = 1,
+              bc: Sequence[int] = (BC_PERIODIC,) * 6, bc_val: Sequence[float] = (0.0,) * 6) -> GridT:
+    g = GridT()
+    g.dim = len(n)
+    n3 = list(n) + [1] * (3 - len(n))
+    d3 = list(d) + [1.0] * (3 - len(d))
+    for i in range(3):
+        g.n[i] = int(n3[i])
+        g.d[i] = float(d3[i])
+    g.ghost = ghost
+    for i in range(6):
+        g.bc_type[i] = int(bc[i])
+        g.bc_val[i] = float(bc_val[i])
+    g.reserved = 0
+    return g
+
+
+def stored_shape(g: GridT):
+    return (g.n[2] + 2 * g.ghost, g.n[1] + 2 * g.ghost, g.n[0] + 2 * g.ghost)
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded libphix_b200.so; raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m phix_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER(C.c_double)
+    G = C.POINTER(GridT)
+    vp = C.c_void_p
+    sig = {
+        "phix_abi_version": ([], C.c_int),
+        "phix_last_error": ([], C.c_char_p),
+        "phix_launch_count": ([], C.c_longlong),
+        "phix_bc_apply": ([vp, G, vp], C.c_int),
+        "phix_lap_accumulate": ([vp, vp, C.c_double, G, vp], C.c_int),
+        "phix_grad_accumulate": ([vp, vp, C.c_double, C.c_int, G, vp], C.c_int),
+        "phix_pointwise_accumulate": ([vp, vp, vp, C.c_double, C.c_int, P, G, vp], C.c_int),
+        "phix_mul_accumulate": ([vp, vp, vp, C.c_double, G, vp], C.c_int),
+        "phix_axpy": ([vp, vp, C.c_double, C.c_size_t, vp], C.c_int),
+        "phix_stepper_create": ([C.POINTER(vp), C.c_int, C.c_int, C.c_int, P, C.c_double, G], C.c_int),
+        "phix_stepper_destroy": ([vp], C.c_int),
+        "phix_stepper_nfields": ([vp], C.c_int),
+        "phix_stepper_load": ([vp, C.POINTER(vp), vp], C.c_int),
+        "phix_stepper_store": ([vp, C.POINTER(vp), vp], C.c_int),
+        "phix_stepper_advance": ([vp, C.c_int, vp], C.c_int),
+        "phix_stepper_set_graph": ([vp, C.c_int], C.c_int),
+        "phix_stepper_bind": ([vp, C.POINTER(vp), C.POINTER(vp)], C.c_int),
+        "phix_stepper_current": ([vp], C.c_int),
+        "phix_stepper_run_host": ([vp, C.POINTER(vp), C.POINTER(vp), C.c_int], C.c_int),
+        "phix_reduce_mass_energy": ([C.POINTER(vp), C.c_int, P, G, P, vp], C.c_int),
+        "phix_stepper_diagnostics": ([vp, P], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(rc: int) -> int:
+    if rc < 0:
+        msg = lib().phix_last_error().decode(errors="replace")
+        if rc == ERR_ARG:
+            raise PhixArgumentError(rc, msg)
+        raise PhixError(rc, msg)
+    return rc
+
+
+def launch_count() -> int:
+    return int(lib().phix_launch_count())
+
+
+def _prm(prm: Sequence[float]):
+    v = list(prm) + [0.0] * (8 - len(prm))
+    return (C.c_double * 8)(*v)
+
+
+def _ptrs(tensors):
+    return (C.c_void_p * len(tensors))(*[t.data_ptr() for t in tensors])
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def _dev(t):
+    import torch
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+        raise PhixArgumentError(ERR_ARG, "expected a contiguous float64 CUDA tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+# ---------------------------------------------------------------------------
+# single operators (device tensors in the stored layout)
+# ---------------------------------------------------------------------------
+def bc_apply(field, g: GridT, stream=None):
+    check(lib().phix_bc_apply(_dev(field), C.byref(g), _stream(stream)))
+
+
+def lap_accumulate(rhs, src, coeff: float, g: GridT, stream=None):
+    check(lib().phix_lap_accumulate(_dev(rhs), _dev(src), coeff, C.byref(g), _stream(stream)))
+
+
+def grad_accumulate(rhs, src, coeff: float, axis: int, g: GridT, stream=None):
+    check(lib().phix_grad_accumulate(_dev(rhs), _dev(src), coeff, axis, C.byref(g), _stream(stream)))
+
+
+def pointwise_accumulate(rhs, s1, s2, coeff: float, func: int, prm: Sequence[float], g: GridT, stream=None):
+    p = _prm(prm)
+    check(lib().phix_pointwise_accumulate(_dev(rhs), _dev(s1), _dev(s2) if s2 is not None else None, coeff,
+                                          func, p, C.byref(g), _stream(stream)))
+
+
+def mul_accumulate(rhs, s1, s2, coeff: float, g: GridT, stream=None):
+    check(lib().phix_mul_accumulate(_dev(rhs), _dev(s1), _dev(s2), coeff, C.byref(g), _stream(stream)))
+
+
+def axpy(dst, src, coeff: float, stream=None):
+    check(lib().phix_axpy(_dev(dst), _dev(src), coeff, dst.numel(), _stream(stream)))
+
+
+def reduce_mass_energy(fields, phys: int, prm: Sequence[float], g: GridT, stream=None):
+    out = (C.c_double * 2)()
+    check(lib().phix_reduce_mass_energy(_ptrs(fields), phys, _prm(prm), C.byref(g), out, _stream(stream)))
+    return out[0], out[1]
+
+
+# ---------------------------------------------------------------------------
+# fused stepper
+# ---------------------------------------------------------------------------
+class Stepper:
+    """Owning wrapper of phix_stepper_t (one built-in physics on one grid)."""
+
+    def __init__(self, phys: int, scheme: int, precision: int, prm: Sequence[float], dt: float, g: GridT):
+        self.g = g
+        self.phys, self.scheme, self.precision = phys, scheme, precision
+        self.prm = list(prm)
+        self.dt = dt
+        h = C.c_void_p()
+        check(lib().phix_stepper_create(C.byref(h), phys, scheme, precision, _prm(prm), dt, C.byref(g)))
+        self.h = h
+        self.nf = NFIELDS[phys]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().phix_stepper_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def load(self, fields, stream=None):
+        check(lib().phix_stepper_load(self.h, _ptrs(fields), _stream(stream)))
+
+    def store(self, fields, stream=None):
+        check(lib().phix_stepper_store(self.h, _ptrs(fields), _stream(stream)))
+
+    def advance(self, nsteps: int, stream=None):
+        check(lib().phix_stepper_advance(self.h, nsteps, _stream(stream)))
+
+    def set_graph(self, steps_per_graph: int):
+        check(lib().phix_stepper_set_graph(self.h, steps_per_graph))
+
+    def bind(self, fields, alt):
+        check(lib().phix_stepper_bind(self.h, _ptrs(fields), _ptrs(alt)))
+
+    def current(self) -> int:
+        return check(lib().phix_stepper_current(self.h))
+
+    def run_host(self, host_in, host_out, nsteps: int):
+        """host_in/host_out: float64 numpy arrays or pinned CPU tensors (stored layout)."""
+        def hp(a):
+            if isinstance(a, np.ndarray):
+                assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+                return a.ctypes.data
+            return a.data_ptr()
+        pin = (C.c_void_p * self.nf)(*[hp(a) for a in host_in])
+        pout = (C.c_void_p * self.nf)(*[hp(a) for a in host_out])
+        check(lib().phix_stepper_run_host(self.h, pin, pout, nsteps))
+
+    def diagnostics(self):
+        out = (C.c_double * 2)()
+        check(lib().phix_stepper_diagnostics(self.h, out))
+        return out[0], out[1]
+
+
+def build_library(verbose: bool = False) -> str:
+    """Compile libphix_b200.so in-tree (nvcc, sm_100a)."""
+    from .build import build as _build
+    return _build(verbose=verbose)

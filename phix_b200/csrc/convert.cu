@@ -1,0 +1,142 @@
+// convert.cu -- moving the stepper state in and out (phix_stepper_load/store,
+// phix_stepper_run_host) and FP64 <-> FP32 conversion of stored arrays.
+#include <cstdint>
+#include <cstring>
+
+#include "common.cuh"
+#include "stepper.h"
+
+namespace phix {
+
+// dst[i] = (float)src[i] over n stored elements, 16-byte vectorised.
+// `vec` = both pointers 16-byte aligned (else scalar).
+__global__ void __launch_bounds__(256) f64_to_f32(float* __restrict__ dst, const double* __restrict__ src, size_t n,
+                                                  int vec) {
+    size_t i = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) * 2;
+    const size_t stride = (size_t)gridDim.x * blockDim.x * 2;
+    if (!vec) {
+        for (size_t j = i / 2; j < n; j += stride / 2) dst[j] = (float)src[j];
+        return;
+    }
+    for (; i + 1 < n; i += stride) {
+        double2 v = *reinterpret_cast<const double2*>(src + i);
+        *reinterpret_cast<float2*>(dst + i) = make_float2((float)v.x, (float)v.y);
+    }
+    if (i < n) dst[i] = (float)src[i];
+}
+__global__ void __launch_bounds__(256) f32_to_f64(double* __restrict__ dst, const float* __restrict__ src, size_t n,
+                                                  int vec) {
+    size_t i = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) * 2;
+    const size_t stride = (size_t)gridDim.x * blockDim.x * 2;
+    if (!vec) {
+        for (size_t j = i / 2; j < n; j += stride / 2) dst[j] = (double)src[j];
+        return;
+    }
+    for (; i + 1 < n; i += stride) {
+        float2 v = *reinterpret_cast<const float2*>(src + i);
+        *reinterpret_cast<double2*>(dst + i) = make_double2((double)v.x, (double)v.y);
+    }
+    if (i < n) dst[i] = (double)src[i];
+}
+
+static int aligned16(const void* a, const void* b) {
+    return ((uintptr_t)a % 16 == 0) && ((uintptr_t)b % 16 == 0);
+}
+
+static int conv_grid(size_t n) {
+    size_t b = (n / 2 + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    return (int)(b ? b : 1);
+}
+
+int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s) {
+    const size_t S = stepper_stored(h);
+    for (int f = 0; f < stepper_nf(h); ++f) {
+        if (!fields[f]) { set_error("load: field %d is NULL", f); return PHIX_ERR_ARG; }
+        // both ping-pong buffers get the full stored array, so ghost layers
+        // that no BC rewrites stay identical whichever buffer is current
+        for (int b = 0; b < 2; ++b) {
+            void* dst = stepper_state_buf(h, b, f);
+            if (stepper_prec(h) == PHIX_F64) {
+                if (dst == (const void*)fields[f]) continue;
+                PHIX_TRY_CUDA(cudaMemcpyAsync(dst, fields[f], S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            } else {
+                f64_to_f32<<<conv_grid(S), 256, 0, s>>>((float*)dst, fields[f], S, aligned16(dst, fields[f]));
+                PHIX_LAUNCH_CHECK("f64_to_f32");
+            }
+        }
+    }
+    return PHIX_OK;
+}
+
+int stepper_copy_out(phix_stepper* h, double* const* fields, cudaStream_t s) {
+    const size_t S = stepper_stored(h);
+    for (int f = 0; f < stepper_nf(h); ++f) {
+        if (!fields[f]) { set_error("store: field %d is NULL", f); return PHIX_ERR_ARG; }
+        const void* src = stepper_state(h, f);
+        if (stepper_prec(h) == PHIX_F64) {
+            if (src == (const void*)fields[f]) continue;
+            PHIX_TRY_CUDA(cudaMemcpyAsync(fields[f], src, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        } else {
+            f32_to_f64<<<conv_grid(S), 256, 0, s>>>(fields[f], (const float*)src, S, aligned16(src, fields[f]));
+            PHIX_LAUNCH_CHECK("f32_to_f64");
+        }
+    }
+    return PHIX_OK;
+}
+
+int stepper_diag(phix_stepper* h, double* out) {
+    const int nf = stepper_nf(h);
+    const int np = reduce_partials_needed(stepper_grid(h));
+    double* part = stepper_partials(h, np);
+    if (!part) { set_error("diagnostics: cudaMalloc failed"); return PHIX_ERR_CUDA; }
+    if (stepper_prec(h) == PHIX_F32) {
+        const float* f[2] = {(const float*)stepper_state(h, 0), nf > 1 ? (const float*)stepper_state(h, 1) : nullptr};
+        return reduce_mass_energy<float>(f, nf, stepper_phys(h), stepper_prm(h), stepper_grid(h), part, np, out, 0);
+    }
+    const double* f[2] = {(const double*)stepper_state(h, 0), nf > 1 ? (const double*)stepper_state(h, 1) : nullptr};
+    return reduce_mass_energy<double>(f, nf, stepper_phys(h), stepper_prm(h), stepper_grid(h), part, np, out, 0);
+}
+
+}  // namespace phix
+
+using namespace phix;
+
+extern "C" {
+
+int phix_stepper_load(phix_stepper_t* h, const double* const* fields, void* stream) {
+    if (!h || !fields) { set_error("load: NULL argument"); return PHIX_ERR_ARG; }
+    return stepper_copy_in(h, fields, (cudaStream_t)stream);
+}
+
+int phix_stepper_store(phix_stepper_t* h, double* const* fields, void* stream) {
+    if (!h || !fields) { set_error("store: NULL argument"); return PHIX_ERR_ARG; }
+    return stepper_copy_out(h, fields, (cudaStream_t)stream);
+}
+
+int phix_stepper_run_host(phix_stepper_t* h, const double* const* host_in, double* const* host_out, int nsteps) {
+    if (!h || !host_in || !host_out || nsteps < 0) { set_error("run_host: bad argument"); return PHIX_ERR_ARG; }
+    const int nf = stepper_nf(h);
+    const size_t S = stepper_stored(h);
+    double* stage = stepper_staging(h);
+    if (!stage) { set_error("run_host: cudaMalloc(staging) failed"); return PHIX_ERR_CUDA; }
+    const double* din[2] = {stage, stage + S};
+    double* dout[2] = {stage, stage + S};
+    for (int f = 0; f < nf; ++f)
+        PHIX_TRY_CUDA(cudaMemcpyAsync(stage + f * S, host_in[f], S * sizeof(double), cudaMemcpyHostToDevice, 0));
+    int rc = stepper_copy_in(h, din, 0);
+    if (rc) return rc;
+    if ((rc = phix_stepper_advance(h, nsteps, 0))) return rc;
+    if ((rc = stepper_copy_out(h, dout, 0))) return rc;
+    for (int f = 0; f < nf; ++f)
+        PHIX_TRY_CUDA(cudaMemcpyAsync(host_out[f], stage + f * S, S * sizeof(double), cudaMemcpyDeviceToHost, 0));
+    PHIX_TRY_CUDA(cudaStreamSynchronize(0));
+    return PHIX_OK;
+}
+
+int phix_stepper_diagnostics(phix_stepper_t* h, double* out) {
+    if (!h || !out) { set_error("diagnostics: NULL argument"); return PHIX_ERR_ARG; }
+    return stepper_diag(h, out);
+}
+
+}  // extern "C"

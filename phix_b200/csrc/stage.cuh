@@ -1,0 +1,397 @@
+// stage.cuh -- fused Runge-Kutta / Euler stage kernels.
+//
+// One launch computes, for every physical cell of its tile,
+//   y   = u + a * k_prev                 (kernel_rk4_tmp, Solver.cu:49-56)
+//   ghost(y) by the field's BCs          (kernel_periodic/noflux/fixed, Boundary.cu:95-195)
+//   rhs = Equation::computeRHS(y)        (Equation.cu:257-276, every DSL term)
+// and writes either k_s = rhs (intermediate RK4 stage) or the new state
+//   RK4  : u + dt/6 (k1 + 2k2 + 2k3 + k4)  (kernel_rk4_update, Solver.cu:61-71)
+//   Euler: u + dt * rhs                    (kernel_axpy, Solver.cu:30-35)
+// The BCs never run as kernels: halo cells of the tile are loaded from the
+// mapped interior cell (periodic wrap, zero-flux clamp) or set to the Dirichlet
+// value.  For lap(expr, bcs) (the Cahn-Hilliard biharmonic) the chemical
+// potential mu is formed in shared memory on the tile plus one ring, with the
+// same BC mapping applied to mu, so mu never touches HBM
+// (makeStencilOnExprTerm, Equation.cu:537-594).
+//
+// Work per launch: 2D/1D use a TX x TY box tile per CTA; 3D uses a TX x TY
+// in-plane tile that marches RZ planes along z with ring buffers of stage-state
+// and mu planes, so every input plane is read once per stage.
+#pragma once
+
+#include "common.cuh"
+
+namespace phix {
+
+enum : int { MODE_K = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2 };
+
+template <typename T>
+struct StageArgs {
+    Layout L;
+    const T* u[2];    // state at the start of the step
+    const T* kin[2];  // previous stage k (nullptr in stage 1 / Euler)
+    const T* k1[2];   // RK4 final stage only
+    const T* k2[2];
+    T* out[2];        // k_s, or the new state in the final modes
+    T a;              // y = u + a * kin
+    T dtf;            // dt/6 (RK4 final) or dt (Euler)
+    T i2[3];          // 1/d^2 per axis
+    T p[8];           // physics coefficients (make_coeffs in stepper.cu)
+};
+
+template <int PHYS> struct PhysTraits;
+template <> struct PhysTraits<PHIX_PHYS_AC> { static constexpr int NF = 1, H = 1; static constexpr bool MU = false; };
+template <> struct PhysTraits<PHIX_PHYS_CH> { static constexpr int NF = 1, H = 2; static constexpr bool MU = true; };
+template <> struct PhysTraits<PHIX_PHYS_CHAC> { static constexpr int NF = 2, H = 2; static constexpr bool MU = true; };
+
+// ---------------------------------------------------------------------------
+// per-cell helpers
+// ---------------------------------------------------------------------------
+
+// Flat stored index of (possibly out-of-domain) coordinates after BC mapping,
+// or MAP_CONST with the constant the ghost fill would have written.
+template <int DIM>
+__device__ __forceinline__ int map3(const Layout& L, int px, int py, int pz, int* idx, double* cval) {
+    int qx, qy = py, qz = pz;
+    if (map_axis(px, L.n[0], L.bc[0], L.bc[1], L.bcv[0], L.bcv[1], L.ghost, &qx, cval) == MAP_CONST) return MAP_CONST;
+    if (DIM >= 2 && map_axis(py, L.n[1], L.bc[2], L.bc[3], L.bcv[2], L.bcv[3], L.ghost, &qy, cval) == MAP_CONST)
+        return MAP_CONST;
+    if (DIM >= 3 && map_axis(pz, L.n[2], L.bc[4], L.bc[5], L.bcv[4], L.bcv[5], L.ghost, &qz, cval) == MAP_CONST)
+        return MAP_CONST;
+    *idx = L.origin + qx + L.s[1] * qy + L.s[2] * qz;
+    return MAP_IN;
+}
+
+// Stage state of field f at (px,py,pz).
+template <typename T, int DIM>
+__device__ __forceinline__ T load_y(const StageArgs<T>& A, int f, int px, int py, int pz, bool interior) {
+    int idx;
+    if (interior) {
+        idx = A.L.origin + px + A.L.s[1] * py + A.L.s[2] * pz;
+    } else {
+        double cval;
+        if (map3<DIM>(A.L, px, py, pz, &idx, &cval) == MAP_CONST) return (T)cval;
+    }
+    T u = __ldg(A.u[f] + idx);
+    if (A.kin[f] == nullptr) return u;
+    return rfma(A.a, __ldg(A.kin[f] + idx), u);
+}
+
+// How mu is obtained at coordinate p along one axis: computed at p (inside or
+// periodic), at the clamped cell (zero-flux), or a constant (Dirichlet value,
+// 0 without BC: the scratch is zeroed and never written there).
+__device__ __forceinline__ int mu_axis(int p, int n, int bc_lo, int bc_hi, double v_lo, double v_hi, int* q,
+                                       double* cval) {
+    if (p >= 0 && p < n) { *q = p; return MAP_IN; }
+    int bc = p < 0 ? bc_lo : bc_hi;
+    if (bc == PHIX_BC_PERIODIC) { *q = p; return MAP_IN; }
+    if (bc == PHIX_BC_NOFLUX) { *q = p < 0 ? 0 : n - 1; return MAP_IN; }
+    *cval = bc == PHIX_BC_FIXED ? (p < 0 ? v_lo : v_hi) : 0.0;
+    return MAP_CONST;
+}
+
+// mu = f'(y) - kappa * lap(y) at tile-local point (lx, ly) of y-plane `yc`
+// (with planes `ym`, `yp` below/above in z for 3D).  W = row pitch of the
+// y tile.  Pointwise term first, then the Laplacian, as in the DSL order.
+template <typename T, int PHYS, int DIM, int W>
+__device__ __forceinline__ T compute_mu(const StageArgs<T>& A, const T* yc0, const T* ym0, const T* yp0,
+                                        const T* yc1, int off) {
+    const T c = yc0[off];
+    const T c2 = rmul((T)2, c);
+    T tx = second_diff(yc0[off + 1], c2, yc0[off - 1]);
+    T ty = DIM >= 2 ? second_diff(yc0[off + W], c2, yc0[off - W]) : (T)0;
+    T tz = DIM >= 3 ? second_diff(yp0[off], c2, ym0[off]) : (T)0;
+    T lap = lap_combine<T, DIM>(tx, ty, tz, A.i2[0], A.i2[1], A.i2[2]);
+    T f;
+    if (PHYS == PHIX_PHYS_CH) f = f_dw(c, A.p[2], A.p[3], A.p[4]);
+    else f = f_chac_c(c, yc1[off], A.p[4]);
+    // scratch = 0; scratch += 1*f; scratch += (-kappa)*lap
+    return rfma(A.p[1], lap, rfma((T)1, f, (T)0));
+}
+
+// Right-hand side of field f at a cell: `m*` are mu planes (CH, CHAC-c) with
+// row pitch MW, `y*` y planes with row pitch W.
+template <typename T, int PHYS, int DIM, int W, int MW>
+__device__ __forceinline__ void compute_rhs(const StageArgs<T>& A, const T* mc, const T* mm, const T* mp, int moff,
+                                            const T* y0c, const T* y0m, const T* y0p, const T* y1c, const T* y1m,
+                                            const T* y1p, int yoff, T* k) {
+    if (PHYS == PHIX_PHYS_AC) {
+        const T p = y0c[yoff];
+        const T p2 = rmul((T)2, p);
+        T tx = second_diff(y0c[yoff + 1], p2, y0c[yoff - 1]);
+        T ty = DIM >= 2 ? second_diff(y0c[yoff + W], p2, y0c[yoff - W]) : (T)0;
+        T tz = DIM >= 3 ? second_diff(y0p[yoff], p2, y0m[yoff]) : (T)0;
+        T lap = lap_combine<T, DIM>(tx, ty, tz, A.i2[0], A.i2[1], A.i2[2]);
+        // rhs = 0; rhs += (L*kappa)*lap; rhs += L*(p - p^3)
+        k[0] = rfma(A.p[1], f_ac(p), rfma(A.p[0], lap, (T)0));
+        return;
+    }
+    {
+        const T m = mc[moff];
+        const T m2 = rmul((T)2, m);
+        T tx = second_diff(mc[moff + 1], m2, mc[moff - 1]);
+        T ty = DIM >= 2 ? second_diff(mc[moff + MW], m2, mc[moff - MW]) : (T)0;
+        T tz = DIM >= 3 ? second_diff(mp[moff], m2, mm[moff]) : (T)0;
+        T lap = lap_combine<T, DIM>(tx, ty, tz, A.i2[0], A.i2[1], A.i2[2]);
+        k[0] = rfma(A.p[0], lap, (T)0);  // rhs = 0; rhs += M*lap(mu)
+    }
+    if (PHYS == PHIX_PHYS_CHAC) {
+        const T e = y1c[yoff];
+        const T e2 = rmul((T)2, e);
+        T tx = second_diff(y1c[yoff + 1], e2, y1c[yoff - 1]);
+        T ty = DIM >= 2 ? second_diff(y1c[yoff + W], e2, y1c[yoff - W]) : (T)0;
+        T tz = DIM >= 3 ? second_diff(y1p[yoff], e2, y1m[yoff]) : (T)0;
+        T lap = lap_combine<T, DIM>(tx, ty, tz, A.i2[0], A.i2[1], A.i2[2]);
+        // rhs = 0; rhs += (-L)*f_eta(eta, c); rhs += (L*kappa_eta)*lap(eta)
+        k[1] = rfma(A.p[2], lap, rfma(A.p[3], f_chac_e(e, y0c[yoff], A.p[4]), (T)0));
+    }
+}
+
+// Writes k or the final state for field f at flat index idx.
+template <typename T, int MODE>
+__device__ __forceinline__ void emit(const StageArgs<T>& A, int f, int idx, T k) {
+    if (MODE == MODE_K) {
+        A.out[f][idx] = k;
+    } else if (MODE == MODE_EULER_FINAL) {
+        A.out[f][idx] = rfma(A.dtf, k, __ldg(A.u[f] + idx));
+    } else {
+        // phi += dt6 * (((k1 + 2 k2) + 2 k3) + k4)
+        T s = radd(__ldg(A.k1[f] + idx), rmul((T)2, __ldg(A.k2[f] + idx)));
+        s = radd(s, rmul((T)2, __ldg(A.kin[f] + idx)));
+        s = radd(s, k);
+        A.out[f][idx] = rfma(A.dtf, s, __ldg(A.u[f] + idx));
+    }
+}
+
+// Ghost cells of the new state: the reference leaves the BC-refreshed ghosts
+// of the old state in place (BCs run at the start of the step and the updates
+// add 0 there), i.e. the mapped value of the OLD state.
+template <typename T, int DIM>
+__device__ __forceinline__ void write_ghost(const StageArgs<T>& A, int nf, int px, int py, int pz) {
+    int src;
+    double cval;
+    int dst = A.L.origin + px + A.L.s[1] * py + A.L.s[2] * pz;
+    bool cst = map3<DIM>(A.L, px, py, pz, &src, &cval) == MAP_CONST;
+    for (int f = 0; f < nf; ++f) A.out[f][dst] = cst ? (T)cval : __ldg(A.u[f] + src);
+}
+
+// ---------------------------------------------------------------------------
+// 1-D / 2-D: box tile
+// ---------------------------------------------------------------------------
+template <typename T, int PHYS, int DIM, int MODE, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) stage_box(const StageArgs<T> A) {
+    using P = PhysTraits<PHYS>;
+    constexpr int NF = P::NF, H = P::H;
+    constexpr int HY = DIM >= 2 ? H : 0;
+    constexpr int WX = TX + 2 * H, WY = TY + 2 * HY;
+    constexpr int MX = TX + 2, MY = TY + (DIM >= 2 ? 2 : 0);
+    __shared__ T ys[NF][WY * WX];
+    __shared__ T ms[P::MU ? MY * MX : 1];
+
+    const int n0 = A.L.n[0], n1 = A.L.n[1];
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const bool interior = x0 - H >= 0 && x0 + TX + H <= n0 && (DIM < 2 || (y0 - HY >= 0 && y0 + TY + HY <= n1));
+
+    for (int i = threadIdx.x; i < WX * WY; i += NT) {
+        const int lx = i % WX, ly = i / WX;
+        const int px = x0 - H + lx, py = y0 - HY + ly;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) ys[f][i] = load_y<T, DIM>(A, f, px, py, 0, interior);
+    }
+    __syncthreads();
+
+    if (P::MU) {
+        for (int i = threadIdx.x; i < MX * MY; i += NT) {
+            const int lx = i % MX, ly = i / MX;
+            const int px = x0 - 1 + lx, py = y0 - (DIM >= 2 ? 1 : 0) + ly;
+            int qx = px, qy = py;
+            double cval = 0.0;
+            bool cst = false;
+            if (!interior) {
+                cst = mu_axis(px, n0, A.L.bc[0], A.L.bc[1], A.L.bcv[0], A.L.bcv[1], &qx, &cval) == MAP_CONST;
+                if (!cst && DIM >= 2)
+                    cst = mu_axis(py, n1, A.L.bc[2], A.L.bc[3], A.L.bcv[2], A.L.bcv[3], &qy, &cval) == MAP_CONST;
+            }
+            T v;
+            if (cst) {
+                v = (T)cval;
+            } else {
+                const int off = (qx - x0 + H) + (qy - y0 + HY) * WX;
+                v = compute_mu<T, PHYS, DIM, WX>(A, ys[0], nullptr, nullptr, ys[NF - 1], off);
+            }
+            ms[i] = v;
+        }
+        __syncthreads();
+    }
+
+    for (int i = threadIdx.x; i < TX * TY; i += NT) {
+        const int lx = i % TX, ly = i / TX;
+        const int px = x0 + lx, py = y0 + ly;
+        if (px >= n0 || (DIM >= 2 && py >= n1)) continue;
+        const int yoff = (lx + H) + (ly + HY) * WX;
+        const int moff = (lx + 1) + (ly + (DIM >= 2 ? 1 : 0)) * MX;
+        T k[2];
+        compute_rhs<T, PHYS, DIM, WX, MX>(A, ms, nullptr, nullptr, moff, ys[0], nullptr, nullptr, ys[NF - 1],
+                                          nullptr, nullptr, yoff, k);
+        const int idx = A.L.origin + px + A.L.s[1] * py;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) emit<T, MODE>(A, f, idx, k[f]);
+    }
+
+    if (MODE != MODE_K && !interior) {
+        const int gl = A.L.ghost;
+        // x faces
+        if (x0 == 0 || x0 + TX >= n0) {
+            for (int i = threadIdx.x; i < TY * gl; i += NT) {
+                const int py = y0 + i / gl, l = 1 + i % gl;
+                if (DIM >= 2 && py >= n1) continue;
+                if (DIM < 2 && i / gl > 0) continue;
+                if (x0 == 0) write_ghost<T, DIM>(A, NF, -l, DIM >= 2 ? py : 0, 0);
+                if (x0 + TX >= n0) write_ghost<T, DIM>(A, NF, n0 - 1 + l, DIM >= 2 ? py : 0, 0);
+            }
+        }
+        if (DIM >= 2 && (y0 == 0 || y0 + TY >= n1)) {
+            for (int i = threadIdx.x; i < TX * gl; i += NT) {
+                const int px = x0 + i % TX, l = 1 + i / TX;
+                if (px >= n0) continue;
+                if (y0 == 0) write_ghost<T, DIM>(A, NF, px, -l, 0);
+                if (y0 + TY >= n1) write_ghost<T, DIM>(A, NF, px, n1 - 1 + l, 0);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3-D: in-plane tile marching along z
+// ---------------------------------------------------------------------------
+template <typename T, int PHYS, int TX, int TY>
+struct March3D {
+    static constexpr int NF = PhysTraits<PHYS>::NF, H = PhysTraits<PHYS>::H;
+    static constexpr int WX = TX + 2 * H, WY = TY + 2 * H, WP = WX * WY;  // y plane
+    static constexpr int MX = TX + 2, MY = TY + 2, MP = MX * MY;         // mu plane
+    static constexpr int NYR = 5, NMR = 4;                               // ring depths
+    static constexpr size_t smem_bytes() {
+        return sizeof(T) * ((size_t)NF * NYR * WP + (PhysTraits<PHYS>::MU ? (size_t)NMR * MP : 0));
+    }
+};
+
+template <typename T, int PHYS, int MODE, int TX, int TY, int RZ, int NT>
+__global__ void __launch_bounds__(NT) stage_march3d(const StageArgs<T> A) {
+    using G = March3D<T, PHYS, TX, TY>;
+    constexpr int NF = G::NF, H = G::H, WX = G::WX, WP = G::WP, MX = G::MX, MP = G::MP;
+    constexpr int NYR = G::NYR, NMR = G::NMR;
+    constexpr bool MU = PhysTraits<PHYS>::MU;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* ysb = reinterpret_cast<T*>(smem_raw);   // [NF][NYR][WP]
+    T* msb = ysb + (size_t)NF * NYR * WP;      // [NMR][MP]
+
+    const int n0 = A.L.n[0], n1 = A.L.n[1], n2 = A.L.n[2];
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * RZ;
+    const int z1 = min(z0 + RZ, n2);
+    const bool in_xy = x0 - H >= 0 && x0 + TX + H <= n0 && y0 - H >= 0 && y0 + TY + H <= n1;
+
+    auto yslot = [&](int f, int z) -> T* { return ysb + ((size_t)f * NYR + (unsigned)(z + 8 * NYR) % NYR) * WP; };
+    auto mslot = [&](int z) -> T* { return msb + (size_t)((unsigned)(z + 8 * NMR) % NMR) * MP; };
+
+    auto form_y = [&](int z) {
+        const bool interior = in_xy && z >= 0 && z < n2;
+        for (int i = threadIdx.x; i < WP; i += NT) {
+            const int lx = i % WX, ly = i / WX;
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+                yslot(f, z)[i] = load_y<T, 3>(A, f, x0 - H + lx, y0 - H + ly, z, interior);
+        }
+    };
+    // mu at plane z (possibly outside the domain along z).
+    auto form_mu = [&](int z) {
+        int qz = z;
+        double zval = 0.0;
+        const bool zconst = mu_axis(z, n2, A.L.bc[4], A.L.bc[5], A.L.bcv[4], A.L.bcv[5], &qz, &zval) == MAP_CONST;
+        T* dst = mslot(z);
+        for (int i = threadIdx.x; i < MP; i += NT) {
+            const int lx = i % MX, ly = i / MX;
+            const int px = x0 - 1 + lx, py = y0 - 1 + ly;
+            int qx = px, qy = py;
+            double cval = zval;
+            bool cst = zconst;
+            if (!cst && !in_xy) {
+                cst = mu_axis(px, n0, A.L.bc[0], A.L.bc[1], A.L.bcv[0], A.L.bcv[1], &qx, &cval) == MAP_CONST;
+                if (!cst) cst = mu_axis(py, n1, A.L.bc[2], A.L.bc[3], A.L.bcv[2], A.L.bcv[3], &qy, &cval) == MAP_CONST;
+            }
+            T v;
+            if (cst) {
+                v = (T)cval;
+            } else {
+                const int off = (qx - x0 + H) + (qy - y0 + H) * WX;
+                v = compute_mu<T, PHYS, 3, WX>(A, yslot(0, qz), yslot(0, qz - 1), yslot(0, qz + 1),
+                                               yslot(NF - 1, qz), off);
+            }
+            dst[i] = v;
+        }
+    };
+
+    // prologue: y planes z0-2 .. z0+1 (z0-1 .. z0 for halo 1), mu planes z0-1, z0
+    for (int z = z0 - H; z < z0 + H; ++z) form_y(z);
+    __syncthreads();
+    if (MU) {
+        form_mu(z0 - 1);
+        form_mu(z0);
+    }
+
+    for (int z = z0; z < z1; ++z) {
+        form_y(z + H);
+        __syncthreads();
+        if (MU) {
+            form_mu(z + 1);
+            __syncthreads();
+        }
+        const T* y0c = yslot(0, z);
+        const T* y0m = yslot(0, z - 1);
+        const T* y0p = yslot(0, z + 1);
+        const T* y1c = yslot(NF - 1, z);
+        const T* y1m = yslot(NF - 1, z - 1);
+        const T* y1p = yslot(NF - 1, z + 1);
+        for (int i = threadIdx.x; i < TX * TY; i += NT) {
+            const int lx = i % TX, ly = i / TX;
+            const int px = x0 + lx, py = y0 + ly;
+            if (px >= n0 || py >= n1) continue;
+            const int yoff = (lx + H) + (ly + H) * WX;
+            const int moff = (lx + 1) + (ly + 1) * MX;
+            T k[2];
+            compute_rhs<T, PHYS, 3, WX, MX>(A, mslot(z), mslot(z - 1), mslot(z + 1), moff, y0c, y0m, y0p, y1c,
+                                            y1m, y1p, yoff, k);
+            const int idx = A.L.origin + px + A.L.s[1] * py + A.L.s[2] * z;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) emit<T, MODE>(A, f, idx, k[f]);
+        }
+        if (MODE != MODE_K) {
+            const int gl = A.L.ghost;
+            if (!in_xy) {
+                if (x0 == 0 || x0 + TX >= n0)
+                    for (int i = threadIdx.x; i < TY * gl; i += NT) {
+                        const int py = y0 + i / gl, l = 1 + i % gl;
+                        if (py >= n1) continue;
+                        if (x0 == 0) write_ghost<T, 3>(A, NF, -l, py, z);
+                        if (x0 + TX >= n0) write_ghost<T, 3>(A, NF, n0 - 1 + l, py, z);
+                    }
+                if (y0 == 0 || y0 + TY >= n1)
+                    for (int i = threadIdx.x; i < TX * gl; i += NT) {
+                        const int px = x0 + i % TX, l = 1 + i / TX;
+                        if (px >= n0) continue;
+                        if (y0 == 0) write_ghost<T, 3>(A, NF, px, -l, z);
+                        if (y0 + TY >= n1) write_ghost<T, 3>(A, NF, px, n1 - 1 + l, z);
+                    }
+            }
+            if (z == 0 || z == n2 - 1)
+                for (int i = threadIdx.x; i < TX * TY * gl; i += NT) {
+                    const int lx = i % TX, ly = (i / TX) % TY, l = 1 + i / (TX * TY);
+                    const int px = x0 + lx, py = y0 + ly;
+                    if (px >= n0 || py >= n1) continue;
+                    if (z == 0) write_ghost<T, 3>(A, NF, px, py, -l);
+                    if (z == n2 - 1) write_ghost<T, 3>(A, NF, px, py, n2 - 1 + l);
+                }
+        }
+    }
+}
+
+}  // namespace phix

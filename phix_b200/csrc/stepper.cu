@@ -1,0 +1,451 @@
+// stepper.cu -- fused time stepper behind phix_stepper_* (Solver / VectorSolver
+// replacement, Solver.cu:86-259, VectorSolver.cu:77-228).
+//
+// RK4 step = 4 launches:
+//   stage 1: k1 = F(u)                       (BCs folded into halo loads)
+//   stage 2: k2 = F(u + dt/2 k1)
+//   stage 3: k3 = F(u + dt/2 k2)
+//   stage 4: u' = u + dt/6 (k1 + 2k2 + 2k3 + F(u + dt k3))   -> other state buffer
+// Euler step = 1 launch: u' = u + dt F(u).
+// The state ping-pongs between two buffers; k buffers are per field.  Groups
+// of steps can be captured once into a CUDA graph and replayed.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "stage.cuh"
+#include "stepper.h"
+
+namespace phix {
+
+// ---------------------------------------------------------------------------
+// launch dispatch
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int BOX_TX = 64, BOX_TY = 16, BOX_NT = 256;
+constexpr int LIN_TX = 256, LIN_NT = 256;
+constexpr int M3_TX = 32, M3_TY = 8, M3_RZ = 16, M3_NT = 256;
+
+template <typename T, int PHYS, int DIM, int MODE>
+int launch_box(const StageArgs<T>& A, cudaStream_t s) {
+    if (DIM == 1) {
+        dim3 grid((A.L.n[0] + LIN_TX - 1) / LIN_TX, 1, 1);
+        stage_box<T, PHYS, 1, MODE, LIN_TX, 1, LIN_NT><<<grid, LIN_NT, 0, s>>>(A);
+    } else {
+        dim3 grid((A.L.n[0] + BOX_TX - 1) / BOX_TX, (A.L.n[1] + BOX_TY - 1) / BOX_TY, 1);
+        stage_box<T, PHYS, 2, MODE, BOX_TX, BOX_TY, BOX_NT><<<grid, BOX_NT, 0, s>>>(A);
+    }
+    PHIX_LAUNCH_CHECK("stage_box");
+    return PHIX_OK;
+}
+
+// Dynamic shared memory of the 3-D kernels is opted in once per stepper
+// creation (never inside a stream capture).
+template <typename T, int PHYS, int MODE>
+int prepare_march() {
+    using G = March3D<T, PHYS, M3_TX, M3_TY>;
+    auto kern = stage_march3d<T, PHYS, MODE, M3_TX, M3_TY, M3_RZ, M3_NT>;
+    PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
+    return PHIX_OK;
+}
+
+template <typename T, int PHYS>
+int prepare_phys() {
+    int rc;
+    if ((rc = prepare_march<T, PHYS, MODE_K>())) return rc;
+    if ((rc = prepare_march<T, PHYS, MODE_RK4_FINAL>())) return rc;
+    return prepare_march<T, PHYS, MODE_EULER_FINAL>();
+}
+
+template <typename T>
+int prepare_t(int phys) {
+    switch (phys) {
+        case PHIX_PHYS_AC: return prepare_phys<T, PHIX_PHYS_AC>();
+        case PHIX_PHYS_CH: return prepare_phys<T, PHIX_PHYS_CH>();
+        default: return prepare_phys<T, PHIX_PHYS_CHAC>();
+    }
+}
+
+template <typename T, int PHYS, int MODE>
+int launch_march(const StageArgs<T>& A, cudaStream_t s) {
+    using G = March3D<T, PHYS, M3_TX, M3_TY>;
+    auto kern = stage_march3d<T, PHYS, MODE, M3_TX, M3_TY, M3_RZ, M3_NT>;
+    const size_t smem = G::smem_bytes();
+    dim3 grid((A.L.n[0] + M3_TX - 1) / M3_TX, (A.L.n[1] + M3_TY - 1) / M3_TY, (A.L.n[2] + M3_RZ - 1) / M3_RZ);
+    kern<<<grid, M3_NT, smem, s>>>(A);
+    PHIX_LAUNCH_CHECK("stage_march3d");
+    return PHIX_OK;
+}
+
+template <typename T, int PHYS, int MODE>
+int launch_dim(int dim, const StageArgs<T>& A, cudaStream_t s) {
+    switch (dim) {
+        case 1: return launch_box<T, PHYS, 1, MODE>(A, s);
+        case 2: return launch_box<T, PHYS, 2, MODE>(A, s);
+        case 3: return launch_march<T, PHYS, MODE>(A, s);
+    }
+    set_error("stage: unsupported dim %d", dim);
+    return PHIX_ERR_ARG;
+}
+
+template <typename T, int PHYS>
+int launch_mode(int dim, int mode, const StageArgs<T>& A, cudaStream_t s) {
+    switch (mode) {
+        case MODE_K: return launch_dim<T, PHYS, MODE_K>(dim, A, s);
+        case MODE_RK4_FINAL: return launch_dim<T, PHYS, MODE_RK4_FINAL>(dim, A, s);
+        case MODE_EULER_FINAL: return launch_dim<T, PHYS, MODE_EULER_FINAL>(dim, A, s);
+    }
+    set_error("stage: bad mode %d", mode);
+    return PHIX_ERR_ARG;
+}
+
+}  // namespace
+
+int prepare_stage(int phys, int dim, int prec) {
+    if (dim != 3) return PHIX_OK;
+    return prec == PHIX_F32 ? prepare_t<float>(phys) : prepare_t<double>(phys);
+}
+
+template <typename T>
+int launch_stage(int phys, int dim, int mode, const StageArgs<T>& A, cudaStream_t s) {
+    switch (phys) {
+        case PHIX_PHYS_AC: return launch_mode<T, PHIX_PHYS_AC>(dim, mode, A, s);
+        case PHIX_PHYS_CH: return launch_mode<T, PHIX_PHYS_CH>(dim, mode, A, s);
+        case PHIX_PHYS_CHAC: return launch_mode<T, PHIX_PHYS_CHAC>(dim, mode, A, s);
+    }
+    set_error("stage: unknown physics %d", phys);
+    return PHIX_ERR_ARG;
+}
+template int launch_stage<float>(int, int, int, const StageArgs<float>&, cudaStream_t);
+template int launch_stage<double>(int, int, int, const StageArgs<double>&, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// grid validation / layout
+// ---------------------------------------------------------------------------
+int validate_grid(const phix_grid_t* g, Layout* L, size_t* stored) {
+    if (!g) { set_error("grid is NULL"); return PHIX_ERR_ARG; }
+    if (g->dim < 1 || g->dim > 3) { set_error("grid.dim must be 1, 2 or 3 (got %d)", g->dim); return PHIX_ERR_ARG; }
+    if (g->ghost < 1) { set_error("grid.ghost must be >= 1 (got %d)", g->ghost); return PHIX_ERR_ARG; }
+    for (int a = 0; a < 3; ++a) {
+        if (g->n[a] < 1) { set_error("grid.n[%d] must be >= 1", a); return PHIX_ERR_ARG; }
+        if (a >= g->dim && g->n[a] != 1) { set_error("grid.n[%d] must be 1 for unused axes", a); return PHIX_ERR_ARG; }
+        if (a < g->dim && !(g->d[a] > 0.0)) { set_error("grid.d[%d] must be > 0", a); return PHIX_ERR_ARG; }
+    }
+    for (int i = 0; i < 6; ++i) {
+        int t = g->bc_type[i];
+        if (t < PHIX_BC_NONE || t > PHIX_BC_FIXED) { set_error("grid.bc_type[%d] invalid (%d)", i, t); return PHIX_ERR_ARG; }
+    }
+    for (int a = 0; a < g->dim; ++a) {
+        bool pl = g->bc_type[2 * a] == PHIX_BC_PERIODIC, ph = g->bc_type[2 * a + 1] == PHIX_BC_PERIODIC;
+        if (pl != ph) {
+            set_error("Periodic BC must be set on both sides of axis %c", "XYZ"[a]);
+            return PHIX_ERR_ARG;
+        }
+    }
+    long long sx = g->n[0] + 2LL * g->ghost, sy = g->n[1] + 2LL * g->ghost, sz = g->n[2] + 2LL * g->ghost;
+    long long S = sx * sy * sz;
+    if (S >= (1LL << 31)) { set_error("stored size %lld exceeds 2^31 elements", S); return PHIX_ERR_ARG; }
+    if (L) {
+        for (int a = 0; a < 3; ++a) L->n[a] = g->n[a];
+        L->s[0] = 1;
+        L->s[1] = (int)sx;
+        L->s[2] = (int)(sx * sy);
+        L->ghost = g->ghost;
+        L->origin = (int)(g->ghost + sx * (g->ghost + sy * g->ghost));
+        for (int i = 0; i < 6; ++i) {
+            // axes beyond dim carry no BC (their ghost planes are never read)
+            L->bc[i] = (i / 2 < g->dim) ? g->bc_type[i] : PHIX_BC_NONE;
+            L->bcv[i] = g->bc_val[i];
+        }
+    }
+    if (stored) *stored = (size_t)S;
+    return PHIX_OK;
+}
+
+int physics_nfields(int phys) { return phys == PHIX_PHYS_CHAC ? 2 : (phys == PHIX_PHYS_AC || phys == PHIX_PHYS_CH) ? 1 : 0; }
+
+// Physics coefficients in kernel precision (rounded from double exactly the
+// way the oracle rounds them).
+template <typename T>
+void make_coeffs(int phys, const double* prm, T* p) {
+    for (int i = 0; i < 8; ++i) p[i] = (T)0;
+    if (phys == PHIX_PHYS_AC) {
+        p[0] = (T)(prm[0] * prm[1]);  // L*kappa (lap)
+        p[1] = (T)prm[0];             // L (pointwise)
+    } else if (phys == PHIX_PHYS_CH) {
+        p[0] = (T)prm[0];              // M
+        p[1] = (T)(-prm[1]);           // -kappa
+        p[2] = (T)2 * (T)prm[2];       // 2 rho
+        p[3] = (T)prm[3];              // ca
+        p[4] = (T)prm[4];              // cb
+    } else {
+        p[0] = (T)prm[0];              // M
+        p[1] = (T)(-prm[2]);           // -kappa_c
+        p[2] = (T)(prm[1] * prm[3]);   // L*kappa_eta
+        p[3] = (T)(-prm[1]);           // -L
+        p[4] = (T)2 * (T)prm[4];       // 2 lambda
+    }
+}
+template void make_coeffs<float>(int, const double*, float*);
+template void make_coeffs<double>(int, const double*, double*);
+
+}  // namespace phix
+
+using namespace phix;
+
+// ---------------------------------------------------------------------------
+// stepper object
+// ---------------------------------------------------------------------------
+struct phix_stepper {
+    int phys = 0, scheme = 0, prec = 0, nf = 1, dim = 2;
+    double prm[8] = {0};
+    double dt = 0.0;
+    phix_grid_t g{};
+    Layout L{};
+    size_t S = 0;      // stored elements per field
+    size_t esz = 8;    // element size of the state
+    void* st[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    bool own_state = true;
+    void* kbuf[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    int cur = 0;
+    cudaStream_t cap = nullptr;
+    int graph_steps = 0;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    double* stage_host = nullptr;  // device FP64 staging for run_host / diagnostics
+    double* partials = nullptr;
+    int partials_n = 0;
+};
+
+namespace phix {
+
+static void drop_graphs(phix_stepper* h) {
+    for (auto& e : h->gexec)
+        if (e) { cudaGraphExecDestroy(e); e = nullptr; }
+}
+
+template <typename T>
+static int enqueue_step(phix_stepper* h, cudaStream_t s) {
+    StageArgs<T> A;
+    memset(&A, 0, sizeof(A));
+    A.L = h->L;
+    for (int a = 0; a < 3; ++a) A.i2[a] = a < h->dim ? (T)(1.0 / (h->g.d[a] * h->g.d[a])) : (T)0;
+    make_coeffs<T>(h->phys, h->prm, A.p);
+    const int c = h->cur, o = 1 - c;
+    for (int f = 0; f < h->nf; ++f) A.u[f] = (const T*)h->st[c][f];
+    int rc;
+    if (h->scheme == PHIX_EULER) {
+        for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->st[o][f];
+        A.dtf = (T)h->dt;
+        rc = launch_stage<T>(h->phys, h->dim, MODE_EULER_FINAL, A, s);
+        if (rc) return rc;
+    } else {
+        const T dt2 = (T)(h->dt * 0.5), dtt = (T)h->dt;
+        // stage 1
+        for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->kbuf[0][f];
+        if ((rc = launch_stage<T>(h->phys, h->dim, MODE_K, A, s))) return rc;
+        // stages 2, 3
+        for (int st = 1; st < 3; ++st) {
+            for (int f = 0; f < h->nf; ++f) {
+                A.kin[f] = (const T*)h->kbuf[st - 1][f];
+                A.out[f] = (T*)h->kbuf[st][f];
+            }
+            A.a = dt2;
+            if ((rc = launch_stage<T>(h->phys, h->dim, MODE_K, A, s))) return rc;
+        }
+        // stage 4 + update
+        for (int f = 0; f < h->nf; ++f) {
+            A.kin[f] = (const T*)h->kbuf[2][f];
+            A.k1[f] = (const T*)h->kbuf[0][f];
+            A.k2[f] = (const T*)h->kbuf[1][f];
+            A.out[f] = (T*)h->st[o][f];
+        }
+        A.a = dtt;
+        A.dtf = (T)(h->dt / 6.0);
+        if ((rc = launch_stage<T>(h->phys, h->dim, MODE_RK4_FINAL, A, s))) return rc;
+    }
+    h->cur = o;
+    return PHIX_OK;
+}
+
+static int enqueue_steps(phix_stepper* h, int n, cudaStream_t s) {
+    for (int i = 0; i < n; ++i) {
+        int rc = h->prec == PHIX_F32 ? enqueue_step<float>(h, s) : enqueue_step<double>(h, s);
+        if (rc) return rc;
+    }
+    return PHIX_OK;
+}
+
+static int replay_group(phix_stepper* h, cudaStream_t s) {
+    const int parity = h->cur;
+    if (!h->gexec[parity]) {
+        cudaGraph_t graph = nullptr;
+        PHIX_TRY_CUDA(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_steps(h, h->graph_steps, h->cap);
+        cudaError_t e = cudaStreamEndCapture(h->cap, &graph);
+        if (rc) { if (graph) cudaGraphDestroy(graph); h->cur = parity; return rc; }
+        if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&h->gexec[parity], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+        h->cur = parity;  // capture only recorded; the replay below advances
+    }
+    PHIX_TRY_CUDA(cudaGraphLaunch(h->gexec[parity], s));
+    // launches inside the graph count as kernel launches of this library
+    count_launch(h->graph_steps * (h->scheme == PHIX_RK4 ? 4 : 1));
+    if (h->graph_steps % 2) h->cur = 1 - parity;
+    return PHIX_OK;
+}
+
+}  // namespace phix
+
+extern "C" {
+
+int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precision, const double* prm, double dt,
+                        const phix_grid_t* g) {
+    if (!out) { set_error("out is NULL"); return PHIX_ERR_ARG; }
+    *out = nullptr;
+    if (physics_nfields(phys) == 0) { set_error("unknown physics %d", phys); return PHIX_ERR_ARG; }
+    if (scheme != PHIX_EULER && scheme != PHIX_RK4) { set_error("unknown scheme %d", scheme); return PHIX_ERR_ARG; }
+    if (precision != PHIX_F32 && precision != PHIX_F64) { set_error("unknown precision %d", precision); return PHIX_ERR_ARG; }
+    if (!prm) { set_error("prm is NULL"); return PHIX_ERR_ARG; }
+    Layout L;
+    size_t S;
+    int rc = validate_grid(g, &L, &S);
+    if (rc) return rc;
+    auto* h = new (std::nothrow) phix_stepper();
+    if (!h) { set_error("out of host memory"); return PHIX_ERR_ARG; }
+    h->phys = phys;
+    h->scheme = scheme;
+    h->prec = precision;
+    h->nf = physics_nfields(phys);
+    h->dim = g->dim;
+    memcpy(h->prm, prm, sizeof(double) * (phys == PHIX_PHYS_AC ? 2 : 5));
+    h->dt = dt;
+    h->g = *g;
+    h->L = L;
+    h->S = S;
+    h->esz = precision == PHIX_F32 ? 4 : 8;
+    auto fail = [&](cudaError_t e, const char* w) {
+        int r = cuda_status(e, w);
+        phix_stepper_destroy(h);
+        return r;
+    };
+    cudaError_t e;
+    for (int b = 0; b < 2; ++b)
+        for (int f = 0; f < h->nf; ++f) {
+            if ((e = cudaMalloc(&h->st[b][f], S * h->esz)) != cudaSuccess) return fail(e, "cudaMalloc(state)");
+            if ((e = cudaMemset(h->st[b][f], 0, S * h->esz)) != cudaSuccess) return fail(e, "cudaMemset(state)");
+        }
+    if (scheme == PHIX_RK4)
+        for (int k = 0; k < 3; ++k)
+            for (int f = 0; f < h->nf; ++f) {
+                // ghosts of k stay zero: kernels only ever write physical cells
+                if ((e = cudaMalloc(&h->kbuf[k][f], S * h->esz)) != cudaSuccess) return fail(e, "cudaMalloc(k)");
+                if ((e = cudaMemset(h->kbuf[k][f], 0, S * h->esz)) != cudaSuccess) return fail(e, "cudaMemset(k)");
+            }
+    if ((e = cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "cudaStreamCreate");
+    if ((rc = prepare_stage(phys, g->dim, precision))) {
+        phix_stepper_destroy(h);
+        return rc;
+    }
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e, "cudaDeviceSynchronize");
+    *out = h;
+    return PHIX_OK;
+}
+
+int phix_stepper_destroy(phix_stepper_t* h) {
+    if (!h) return PHIX_OK;
+    drop_graphs(h);
+    if (h->own_state)
+        for (auto& b : h->st)
+            for (auto& p : b)
+                if (p) cudaFree(p);
+    for (auto& k : h->kbuf)
+        for (auto& p : k)
+            if (p) cudaFree(p);
+    if (h->stage_host) cudaFree(h->stage_host);
+    if (h->partials) cudaFree(h->partials);
+    if (h->cap) cudaStreamDestroy(h->cap);
+    delete h;
+    return PHIX_OK;
+}
+
+int phix_stepper_nfields(const phix_stepper_t* h) { return h ? h->nf : 0; }
+
+int phix_stepper_current(const phix_stepper_t* h) { return h ? h->cur : -1; }
+
+int phix_stepper_set_graph(phix_stepper_t* h, int steps_per_graph) {
+    if (!h || steps_per_graph < 0) { set_error("bad stepper or steps_per_graph"); return PHIX_ERR_ARG; }
+    drop_graphs(h);
+    h->graph_steps = steps_per_graph;
+    return PHIX_OK;
+}
+
+int phix_stepper_bind(phix_stepper_t* h, double* const* fields, double* const* alt) {
+    if (!h || !fields || !alt) { set_error("bind: NULL argument"); return PHIX_ERR_ARG; }
+    if (h->prec != PHIX_F64) { set_error("bind: only FP64 steppers run on caller buffers"); return PHIX_ERR_UNSUPPORTED; }
+    for (int f = 0; f < h->nf; ++f)
+        if (!fields[f] || !alt[f] || fields[f] == alt[f]) { set_error("bind: field %d buffers invalid", f); return PHIX_ERR_ARG; }
+    drop_graphs(h);
+    if (h->own_state)
+        for (auto& b : h->st)
+            for (auto& p : b)
+                if (p) { cudaFree(p); p = nullptr; }
+    h->own_state = false;
+    for (int f = 0; f < h->nf; ++f) {
+        h->st[0][f] = fields[f];
+        h->st[1][f] = alt[f];
+    }
+    h->cur = 0;
+    return PHIX_OK;
+}
+
+int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream) {
+    if (!h || nsteps < 0) { set_error("advance: bad stepper or nsteps"); return PHIX_ERR_ARG; }
+    if (!h->st[0][0]) { set_error("advance: stepper has no state buffers"); return PHIX_ERR_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc;
+    if (h->graph_steps > 0) {
+        while (nsteps >= h->graph_steps) {
+            if ((rc = replay_group(h, s))) return rc;
+            nsteps -= h->graph_steps;
+        }
+    }
+    return enqueue_steps(h, nsteps, s);
+}
+
+}  // extern "C"
+
+// state conversion lives in convert.cu (needs a kernel)
+namespace phix {
+int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s);
+int stepper_copy_out(phix_stepper* h, double* const* fields, cudaStream_t s);
+int stepper_diag(phix_stepper* h, double* out);
+void* stepper_state(phix_stepper* h, int f) { return h->st[h->cur][f]; }
+void* stepper_state_buf(phix_stepper* h, int b, int f) { return h->st[b][f]; }
+size_t stepper_stored(const phix_stepper* h) { return h->S; }
+int stepper_prec(const phix_stepper* h) { return h->prec; }
+int stepper_nf(const phix_stepper* h) { return h->nf; }
+int stepper_phys(const phix_stepper* h) { return h->phys; }
+const phix_grid_t* stepper_grid(const phix_stepper* h) { return &h->g; }
+const double* stepper_prm(const phix_stepper* h) { return h->prm; }
+double* stepper_staging(phix_stepper* h) {
+    if (!h->stage_host) {
+        if (cudaMalloc(&h->stage_host, h->S * sizeof(double) * h->nf) != cudaSuccess) return nullptr;
+    }
+    return h->stage_host;
+}
+double* stepper_partials(phix_stepper* h, int n) {
+    if (h->partials_n < n) {
+        if (h->partials) cudaFree(h->partials);
+        h->partials = nullptr;
+        h->partials_n = 0;
+        if (cudaMalloc(&h->partials, sizeof(double) * n) != cudaSuccess) return nullptr;
+        h->partials_n = n;
+    }
+    return h->partials;
+}
+}  // namespace phix

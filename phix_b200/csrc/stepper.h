@@ -1,0 +1,38 @@
+// stepper.h -- internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "../../include/phix_b200.h"
+#include "common.cuh"
+
+namespace phix {
+
+template <typename T> struct StageArgs;
+
+int validate_grid(const phix_grid_t* g, Layout* L, size_t* stored);
+int physics_nfields(int phys);
+template <typename T> void make_coeffs(int phys, const double* prm, T* p);
+int prepare_stage(int phys, int dim, int prec);
+template <typename T> int launch_stage(int phys, int dim, int mode, const StageArgs<T>& A, cudaStream_t s);
+
+// accessors into the opaque stepper (stepper.cu)
+void* stepper_state(phix_stepper* h, int f);
+void* stepper_state_buf(phix_stepper* h, int b, int f);
+size_t stepper_stored(const phix_stepper* h);
+int stepper_prec(const phix_stepper* h);
+int stepper_nf(const phix_stepper* h);
+int stepper_phys(const phix_stepper* h);
+const phix_grid_t* stepper_grid(const phix_stepper* h);
+const double* stepper_prm(const phix_stepper* h);
+double* stepper_staging(phix_stepper* h);
+double* stepper_partials(phix_stepper* h, int n);
+
+// diagnostics core (reduce.cu): fields in precision T, FP64 accumulation.
+template <typename T>
+int reduce_mass_energy(const T* const* fields, int nf, int phys, const double* prm, const phix_grid_t* g,
+                       double* partials, int partials_n, double* out, cudaStream_t s);
+int reduce_partials_needed(const phix_grid_t* g);
+
+}  // namespace phix

@@ -1,0 +1,87 @@
+"""Parity with the reference's own GPU build on the B200, at the benchmark
+configurations' full sizes and step counts.
+
+oracle/_ref/libphix_ref.so is the reference library compiled from its sources
+for sm_100a (oracle/Makefile); its Solver / VectorSolver run on the same
+device from the same seeded inputs.  Bar: max-abs <= 1e-12 on every physical
+cell after the stated step count (FP64).  Skipped when oracle/_ref was not
+built (no reference tree where the library was built).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import phix_b200 as px
+from phix_b200 import workloads
+from oracle.oracle import Grid
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def ogrid(g):
+    return Grid(n=tuple(g.n[a] for a in range(g.dim)), d=tuple(g.d[a] for a in range(g.dim)), ghost=g.ghost,
+                bc=tuple(g.bc_type), bc_val=tuple(g.bc_val))
+
+
+def run_mine(g, phys, prm, scheme, dt, nsteps, fields, precision=px.F64, graph=50):
+    st = px.Stepper(phys, scheme, precision, prm, dt, g)
+    d = [torch.from_numpy(f).cuda() for f in fields]
+    st.load(d)
+    if graph:
+        st.set_graph(graph)
+    st.advance(nsteps)
+    st.store(d)
+    torch.cuda.synchronize()
+    st.close()
+    return [x.cpu().numpy() for x in d]
+
+
+def maxdiff(grid, a, b):
+    return max(np.abs(grid.phys(x) - grid.phys(y)).max() for x, y in zip(a, b))
+
+
+@pytest.mark.parametrize("path", sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz")) if "multistep" not in p),
+                         ids=lambda p: os.path.basename(p)[:-4])
+def test_golden_cases_vs_reference_gpu(cuda, reference, path):
+    z = np.load(path)
+    n = tuple(int(v) for v in z["n"])
+    g = px.make_grid(n, tuple(float(v) for v in z["d"]), int(z["ghost"]), tuple(int(v) for v in z["bc"]),
+                     tuple(float(v) for v in z["bc_val"]))
+    grid = ogrid(g)
+    ref = [np.ascontiguousarray(a) for a in z["inputs"]]
+    reference.advance(ref, int(z["phys"]), list(z["prm"]), int(z["scheme"]), float(z["dt"]), int(z["nsteps"]), grid,
+                      use_gpu=True)
+    mine = run_mine(g, int(z["phys"]), list(z["prm"]), int(z["scheme"]), float(z["dt"]), int(z["nsteps"]),
+                    [np.ascontiguousarray(a) for a in z["inputs"]], graph=0)
+    d = maxdiff(grid, mine, ref)
+    print(f"{os.path.basename(path)}: max-abs vs reference GPU = {d:.3e}")
+    assert d <= 1e-12
+
+
+@pytest.mark.parametrize("name", ["ac2d", "ch2d"])
+def test_full_size_config_vs_reference_gpu(cuda, reference, name):
+    g, phys, prm, scheme, dt, nsteps, fields = getattr(workloads, name)()
+    grid = ogrid(g)
+    ref = [f.copy() for f in fields]
+    ms = reference.advance(ref, phys, prm, scheme, dt, nsteps, grid, use_gpu=True)
+    mine = run_mine(g, phys, prm, scheme, dt, nsteps, [f.copy() for f in fields])
+    d = maxdiff(grid, mine, ref)
+    print(f"{name} {g.n[0]}^{g.dim} x {nsteps} steps: max-abs vs reference GPU = {d:.3e} "
+          f"(reference {ms / nsteps * 1e3:.1f} us/step)")
+    assert d <= 1e-12
+
+
+def test_full_size_chac3d_vs_reference_gpu(cuda, reference):
+    g, phys, prm, scheme, dt, nsteps, fields = workloads.chac3d()
+    grid = ogrid(g)
+    ref = [f.copy() for f in fields]
+    ms = reference.advance(ref, phys, prm, scheme, dt, nsteps, grid, use_gpu=True)
+    mine = run_mine(g, phys, prm, scheme, dt, nsteps, [f.copy() for f in fields])
+    d = maxdiff(grid, mine, ref)
+    print(f"chac3d 256^3 x {nsteps}: max-abs vs reference GPU = {d:.3e} (reference {ms / nsteps:.3f} ms/step)")
+    assert d <= 1e-12

@@ -1,0 +1,150 @@
+"""Parity of the fused sm_100a stepper (phix_stepper_*) on a B200.
+
+For every golden case (tests/golden, produced by the reference library's own
+CPU path):
+  * FP64 kernels vs the oracle in fma_mode 1 (the contracted multiply-adds the
+    kernels pin with __fma_rn): identical bits in every stored cell that the
+    reference defines (physical cells, ghost faces, untouched padding planes;
+    ghost corners excluded, they depend on the order of the BC objects).
+  * FP64 kernels vs the reference's CPU vectors: max-abs <= 1e-12 (the two
+    differ only by FMA contraction).
+  * FP32 kernels vs the FP32 oracle: identical bits on physical cells.
+Graph replay, caller-owned buffers (bind) and host buffers (run_host) must
+give the same bits as plain launches.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import phix_b200 as px
+from oracle.oracle import Grid
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+CASES = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz")) if "multistep" not in p)
+IDS = [os.path.basename(p)[:-4] for p in CASES]
+
+
+def load(path):
+    z = np.load(path)
+    n = tuple(int(v) for v in z["n"])
+    d = tuple(float(v) for v in z["d"])
+    bc = tuple(int(v) for v in z["bc"])
+    bcv = tuple(float(v) for v in z["bc_val"])
+    grid = Grid(n=n, d=d, ghost=int(z["ghost"]), bc=bc, bc_val=bcv)
+    g = px.make_grid(n, d, int(z["ghost"]), bc, bcv)
+    return z, grid, g
+
+
+def corner_mask(grid):
+    """True on cells that lie outside the physical range on 2+ active axes."""
+    sh = grid.stored_shape
+    gh = grid.ghost
+    n0, n1, n2 = grid.n3
+    out = np.zeros(sh, dtype=np.int8)
+    ranges = [(2, n0), (1, n1), (0, n2)][:grid.dim]
+    for axis, n in ranges:
+        idx = np.arange(sh[axis])
+        o = ((idx < gh) | (idx >= gh + n)).astype(np.int8)
+        shape = [1, 1, 1]
+        shape[axis] = sh[axis]
+        out = out + o.reshape(shape)
+    return out >= 2
+
+
+def run_gpu(z, g, precision, graph=0, bind=False, nsteps=None):
+    phys, scheme = int(z["phys"]), int(z["scheme"])
+    st = px.Stepper(phys, scheme, precision, list(z["prm"]), float(z["dt"]), g)
+    fields = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in z["inputs"]]
+    n = int(z["nsteps"]) if nsteps is None else nsteps
+    if graph:
+        st.set_graph(graph)
+    if bind:
+        alt = [f.clone() for f in fields]
+        st.bind(fields, alt)
+        st.advance(n)
+        torch.cuda.synchronize()
+        cur = st.current()
+        res = [(alt if cur else fields)[f].cpu().numpy() for f in range(len(fields))]
+    else:
+        st.load(fields)
+        st.advance(n)
+        outs = [torch.empty_like(f) for f in fields]
+        st.store(outs)
+        torch.cuda.synchronize()
+        res = [o.cpu().numpy() for o in outs]
+    st.close()
+    return res
+
+
+@pytest.mark.parametrize("path", CASES, ids=IDS)
+def test_fp64_bitwise_vs_oracle_and_close_to_reference(cuda, oracle, path):
+    z, grid, g = load(path)
+    got = run_gpu(z, g, px.F64)
+    want = [np.ascontiguousarray(a) for a in z["inputs"]]
+    oracle.advance(want, int(z["phys"]), list(z["prm"]), int(z["scheme"]), float(z["dt"]), int(z["nsteps"]),
+                   grid, fma_mode=1)
+    keep = ~corner_mask(grid)
+    for a, b, r in zip(got, want, z["outputs"]):
+        assert np.array_equal(a[keep], b[keep]), f"kernel vs oracle max diff {np.abs(a - b)[keep].max()}"
+        assert np.abs(grid.phys(a) - grid.phys(r)).max() <= 1e-12
+
+
+@pytest.mark.parametrize("path", CASES, ids=IDS)
+def test_fp32_bitwise_vs_fp32_oracle(cuda, oracle, path):
+    z, grid, g = load(path)
+    got = run_gpu(z, g, px.F32)
+    want = [np.ascontiguousarray(a).astype(np.float32) for a in z["inputs"]]
+    oracle.advance(want, int(z["phys"]), list(z["prm"]), int(z["scheme"]), float(z["dt"]), int(z["nsteps"]),
+                   grid, fma_mode=1)
+    for a, b, r in zip(got, want, z["outputs"]):
+        pa, pb = grid.phys(a), grid.phys(b).astype(np.float64)
+        assert np.array_equal(pa, pb), f"max diff {np.abs(pa - pb).max()}"
+        # and FP32 stays close to the FP64 reference on these short runs
+        assert np.abs(pa - grid.phys(r)).max() < 1e-4
+
+
+@pytest.mark.parametrize("path", [p for p in CASES if "ch2d_rk4.npz" in p or "chac3d_rk4.npz" in p
+                                  or "ac2d_euler" in p])
+def test_graph_and_bind_paths_identical(cuda, path):
+    z, grid, g = load(path)
+    base = run_gpu(z, g, px.F64)
+    for graph, bind in ((3, False), (4, False), (0, True), (5, True)):
+        other = run_gpu(z, g, px.F64, graph=graph, bind=bind)
+        for a, b in zip(base, other):
+            assert np.array_equal(grid.phys(a), grid.phys(b)), (graph, bind)
+
+
+def test_run_host_matches_device_path(cuda):
+    z, grid, g = load(os.path.join(GOLDEN, "ch2d_rk4.npz"))
+    base = run_gpu(z, g, px.F64)
+    st = px.Stepper(int(z["phys"]), int(z["scheme"]), px.F64, list(z["prm"]), float(z["dt"]), g)
+    hin = [np.ascontiguousarray(a) for a in z["inputs"]]
+    hout = [np.empty_like(a) for a in hin]
+    st.run_host(hin, hout, int(z["nsteps"]))
+    st.close()
+    assert np.array_equal(grid.phys(hout[0]), grid.phys(base[0]))
+
+
+def test_zero_steps_is_identity(cuda):
+    z, grid, g = load(os.path.join(GOLDEN, "chac3d_rk4.npz"))
+    got = run_gpu(z, g, px.F64, nsteps=0)
+    for a, b in zip(got, z["inputs"]):
+        assert np.array_equal(a, b)
+
+
+def test_launch_counter_counts_stage_kernels(cuda):
+    z, grid, g = load(os.path.join(GOLDEN, "ch2d_rk4.npz"))
+    st = px.Stepper(px.PHYS_CH, px.RK4, px.F64, list(z["prm"]), float(z["dt"]), g)
+    f = [torch.from_numpy(np.ascontiguousarray(z["inputs"][0])).cuda()]
+    st.load(f)
+    torch.cuda.synchronize()
+    before = px.launch_count()
+    st.advance(7)
+    torch.cuda.synchronize()
+    assert px.launch_count() - before == 7 * 4
+    st.close()
