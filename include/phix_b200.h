@@ -55,6 +55,12 @@ extern "C" {
 /* time schemes (Solver.h:17-20) */
 #define PHIX_EULER 0
 #define PHIX_RK4 1
+/* Multi-step Euler of the shipped Cahn-Hilliard app (PHIX_PHYS_CH only, 1-D/2-D,
+ * ghost 1): fields (c, mu); per step mu = f'(c) - kappa*lap(c) (STEADY) and
+ * c += dt*M*lap(mu) (TRANSIENT), one launch.  Replaces Solver(steps, dt) with
+ * {&c, bcs, &eqMu, STEADY}, {&mu, bcs, &eqC, TRANSIENT} (Solver.cu:112-144,
+ * :317-340).  mu always stays in the caller's / first buffer. */
+#define PHIX_MULTISTEP 2
 
 /* arithmetic of the stencil kernels */
 #define PHIX_F64 0
@@ -159,6 +165,35 @@ int phix_stepper_current(const phix_stepper_t* h);
 /* End-to-end convenience: host FP64 stored arrays in, nsteps, host arrays
  * out (host->device copy, advance, device->host copy, synchronise). */
 int phix_stepper_run_host(phix_stepper_t* h, const double* const* host_in, double* const* host_out, int nsteps);
+
+/* ---- batched engine: many independent 2-D fields in one launch per stage */
+
+typedef struct phix_batch phix_batch_t;
+
+/* ninst independent 2-D simulations of one single-field physics (AC or CH),
+ * each with its own grid (size, spacing, BCs) and its own prm[8*i .. 8*i+7],
+ * advanced in lockstep with time step dt.  Each RK stage of all instances is
+ * one persistent kernel over a shared tile list; state and stage buffers come
+ * from one device pool.  No reference counterpart: the reference runs one
+ * Solver per field (Solver.cu:86-107), i.e. instances one after another. */
+int phix_batch_create(phix_batch_t** out, int phys, int scheme, int precision, int ninst, const phix_grid_t* grids,
+                      const double* prm, double dt);
+int phix_batch_destroy(phix_batch_t* b);
+/* Copy one instance's FP64 stored array in / out (device, or host when
+ * from_host / to_host is non-zero; host copies are synchronous). */
+int phix_batch_load(phix_batch_t* b, int inst, const double* field, int from_host, void* stream);
+int phix_batch_store(phix_batch_t* b, int inst, double* field, int to_host, void* stream);
+int phix_batch_advance(phix_batch_t* b, int nsteps, void* stream);
+int phix_batch_set_graph(phix_batch_t* b, int steps_per_graph);
+/* Tile shape id (0..5: 64x16, 32x16, 128x8, 64x8, 32x32, 128x16) and resident
+ * CTAs per SM of the persistent launches (0 = occupancy limit). */
+int phix_batch_set_tiles(phix_batch_t* b, int tile_cfg, int ctas_per_sm);
+int phix_batch_get_tiles(const phix_batch_t* b, int* tile_cfg, int* ctas_per_sm, int* ntiles);
+/* Time every tile shape x CTA count on trial_steps steps of the real batch
+ * (state saved and restored), keep the fastest; *best_ms = ms per step. */
+int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms);
+/* FP64 mass (sum of u * dV over physical cells) per instance; synchronous. */
+int phix_batch_mass(phix_batch_t* b, double* masses);
 
 /* ---- diagnostics (FP64 accumulation) ----------------------------------- */
 

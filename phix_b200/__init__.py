@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "libphix_b200.so")
 OK, ERR_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2, -3, -4
 BC_NONE, BC_PERIODIC, BC_NOFLUX, BC_FIXED = 0, 1, 2, 3
 PHYS_AC, PHYS_CH, PHYS_CHAC = 0, 1, 2
-EULER, RK4 = 0, 1
+EULER, RK4, MULTISTEP = 0, 1, 2
 F64, F32 = 0, 1
 PW_IDENT, PW_AC, PW_DW, PW_CHAC_C, PW_CHAC_E, PW_MUL = range(6)
 
@@ -108,6 +108,16 @@ def lib() -> C.CDLL:
         "phix_stepper_current": ([vp], C.c_int),
         "phix_stepper_run_host": ([vp, C.POINTER(vp), C.POINTER(vp), C.c_int], C.c_int),
         "phix_reduce_mass_energy": ([C.POINTER(vp), C.c_int, P, G, P, vp], C.c_int),
+        "phix_batch_create": ([C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_int, G, P, C.c_double], C.c_int),
+        "phix_batch_destroy": ([vp], C.c_int),
+        "phix_batch_load": ([vp, C.c_int, vp, C.c_int, vp], C.c_int),
+        "phix_batch_store": ([vp, C.c_int, vp, C.c_int, vp], C.c_int),
+        "phix_batch_advance": ([vp, C.c_int, vp], C.c_int),
+        "phix_batch_set_graph": ([vp, C.c_int], C.c_int),
+        "phix_batch_set_tiles": ([vp, C.c_int, C.c_int], C.c_int),
+        "phix_batch_get_tiles": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "phix_batch_autotune": ([vp, C.c_int, P], C.c_int),
+        "phix_batch_mass": ([vp, P], C.c_int),
         "phix_stepper_diagnostics": ([vp, P], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -254,6 +264,73 @@ class Stepper:
         out = (C.c_double * 2)()
         check(lib().phix_stepper_diagnostics(self.h, out))
         return out[0], out[1]
+
+
+class Batch:
+    """Owning wrapper of phix_batch_t: many independent 2-D fields of one
+    single-field physics advanced in lockstep, one persistent launch per stage."""
+
+    def __init__(self, phys: int, scheme: int, precision: int, grids, prms, dt: float):
+        self.n = len(grids)
+        self.grids = list(grids)
+        garr = (GridT * self.n)(*grids)
+        flat = []
+        for p in prms:
+            flat += list(p) + [0.0] * (8 - len(p))
+        parr = (C.c_double * len(flat))(*flat)
+        h = C.c_void_p()
+        check(lib().phix_batch_create(C.byref(h), phys, scheme, precision, self.n, garr, parr, dt))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().phix_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, inst: int, field, stream=None):
+        """field: FP64 stored array; numpy (host) or CUDA tensor (device)."""
+        if isinstance(field, np.ndarray):
+            assert field.dtype == np.float64 and field.flags["C_CONTIGUOUS"]
+            check(lib().phix_batch_load(self.h, inst, C.c_void_p(field.ctypes.data), 1, _stream(stream)))
+        else:
+            check(lib().phix_batch_load(self.h, inst, _dev(field), 0, _stream(stream)))
+
+    def store(self, inst: int, field, stream=None):
+        if isinstance(field, np.ndarray):
+            assert field.dtype == np.float64 and field.flags["C_CONTIGUOUS"]
+            check(lib().phix_batch_store(self.h, inst, C.c_void_p(field.ctypes.data), 1, _stream(stream)))
+        else:
+            check(lib().phix_batch_store(self.h, inst, _dev(field), 0, _stream(stream)))
+
+    def advance(self, nsteps: int, stream=None):
+        check(lib().phix_batch_advance(self.h, nsteps, _stream(stream)))
+
+    def set_graph(self, steps: int):
+        check(lib().phix_batch_set_graph(self.h, steps))
+
+    def set_tiles(self, cfg: int, ctas_per_sm: int = 0):
+        check(lib().phix_batch_set_tiles(self.h, cfg, ctas_per_sm))
+
+    def tiles(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().phix_batch_get_tiles(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def autotune(self, trial_steps: int = 5) -> float:
+        ms = C.c_double()
+        check(lib().phix_batch_autotune(self.h, trial_steps, C.byref(ms)))
+        return ms.value
+
+    def mass(self):
+        out = (C.c_double * self.n)()
+        check(lib().phix_batch_mass(self.h, out))
+        return list(out)
 
 
 def build_library(verbose: bool = False) -> str:

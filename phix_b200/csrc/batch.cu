@@ -1,0 +1,541 @@
+// batch.cu -- many independent simulations of uneven grid sizes and
+// parameters in one persistent launch per RK stage (phix_batch_*).
+//
+// All instances share physics, scheme, precision and dim (2-D), and advance in
+// lockstep.  Each has its own stored layout, BCs, coefficients, two state
+// buffers and k1..k3, carved from one device pool.  A stage launch is one
+// persistent kernel (stage_box_batched) over a tile list covering every
+// instance (largest instances first), with per-instance StageArgs prepared
+// once on the host for each (stage, parity) pair.  Groups of steps are
+// captured into a CUDA graph.  The tile shape and the number of resident CTAs
+// per SM are chosen by a measuring autotuner (phix_batch_autotune).
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "stage.cuh"
+#include "stepper.h"
+
+namespace phix {
+namespace {
+
+struct TileCfg {
+    int tx, ty, nt;
+};
+// Candidate tile shapes (index = PHIX tile config id).
+constexpr TileCfg kTileCfgs[] = {{64, 16, 256}, {32, 16, 256}, {128, 8, 256}, {64, 8, 256}, {32, 32, 256}, {128, 16, 256}};
+constexpr int kNumTileCfgs = sizeof(kTileCfgs) / sizeof(kTileCfgs[0]);
+
+template <typename T, int PHYS, int MODE, int TX, int TY, int NT>
+int launch_batched_cfg(const StageArgs<T>* args, const BatchTile* tiles, int ntiles, int ctas_per_sm, int nsm,
+                       cudaStream_t s) {
+    auto kern = stage_box_batched<T, PHYS, MODE, TX, TY, NT>;
+    int occ = 0;
+    PHIX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, 0));
+    int per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, std::max(occ, 1)) : std::max(occ, 1);
+    int grid = std::min(ntiles, nsm * per_sm);
+    if (grid < 1) grid = 1;
+    kern<<<grid, NT, 0, s>>>(args, tiles, ntiles);
+    PHIX_LAUNCH_CHECK("stage_box_batched");
+    return PHIX_OK;
+}
+
+template <typename T, int PHYS, int MODE>
+int launch_batched_mode(int cfg, const StageArgs<T>* args, const BatchTile* tiles, int ntiles, int cps, int nsm,
+                        cudaStream_t s) {
+    switch (cfg) {
+        case 0: return launch_batched_cfg<T, PHYS, MODE, 64, 16, 256>(args, tiles, ntiles, cps, nsm, s);
+        case 1: return launch_batched_cfg<T, PHYS, MODE, 32, 16, 256>(args, tiles, ntiles, cps, nsm, s);
+        case 2: return launch_batched_cfg<T, PHYS, MODE, 128, 8, 256>(args, tiles, ntiles, cps, nsm, s);
+        case 3: return launch_batched_cfg<T, PHYS, MODE, 64, 8, 256>(args, tiles, ntiles, cps, nsm, s);
+        case 4: return launch_batched_cfg<T, PHYS, MODE, 32, 32, 256>(args, tiles, ntiles, cps, nsm, s);
+        case 5: return launch_batched_cfg<T, PHYS, MODE, 128, 16, 256>(args, tiles, ntiles, cps, nsm, s);
+    }
+    set_error("batch: bad tile config %d", cfg);
+    return PHIX_ERR_ARG;
+}
+
+template <typename T, int PHYS>
+int launch_batched_phys(int mode, int cfg, const StageArgs<T>* args, const BatchTile* tiles, int ntiles, int cps,
+                        int nsm, cudaStream_t s) {
+    switch (mode) {
+        case MODE_K: return launch_batched_mode<T, PHYS, MODE_K>(cfg, args, tiles, ntiles, cps, nsm, s);
+        case MODE_RK4_FINAL: return launch_batched_mode<T, PHYS, MODE_RK4_FINAL>(cfg, args, tiles, ntiles, cps, nsm, s);
+        default: return launch_batched_mode<T, PHYS, MODE_EULER_FINAL>(cfg, args, tiles, ntiles, cps, nsm, s);
+    }
+}
+
+template <typename T>
+int launch_batched(int phys, int mode, int cfg, const StageArgs<T>* args, const BatchTile* tiles, int ntiles, int cps,
+                   int nsm, cudaStream_t s) {
+    switch (phys) {
+        case PHIX_PHYS_AC: return launch_batched_phys<T, PHIX_PHYS_AC>(mode, cfg, args, tiles, ntiles, cps, nsm, s);
+        case PHIX_PHYS_CH: return launch_batched_phys<T, PHIX_PHYS_CH>(mode, cfg, args, tiles, ntiles, cps, nsm, s);
+    }
+    set_error("batch: physics %d not supported", phys);
+    return PHIX_ERR_UNSUPPORTED;
+}
+
+// Per-tile FP64 sums of field 0 over physical cells; then per-instance sums of
+// the tile partials in list order (deterministic).
+template <typename T>
+__global__ void __launch_bounds__(256) batch_tile_mass(const StageArgs<T>* __restrict__ args,
+                                                       const BatchTile* __restrict__ tiles, int ntiles, int tx, int ty,
+                                                       double* __restrict__ part) {
+    __shared__ double sh[8];
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const BatchTile bt = tiles[t];
+        const StageArgs<T>& A = args[bt.inst];
+        double s = 0.0;
+        for (int i = threadIdx.x; i < tx * ty; i += 256) {
+            const int px = bt.x0 + i % tx, py = bt.y0 + i / tx;
+            if (px < A.L.n[0] && py < A.L.n[1]) s += (double)A.u[0][A.L.origin + px + A.L.s[1] * py];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v = 0.0;
+            for (int w = 0; w < 8; ++w) v += sh[w];
+            part[t] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// se[i] = first tile of instance i, se[ninst + 1 + i] = one past its last.
+__global__ void batch_inst_sum(const double* __restrict__ part, const int* __restrict__ se, int ninst,
+                               const double* __restrict__ dv, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ninst) return;
+    double s = 0.0;
+    for (int t = se[i]; t < se[ninst + 1 + i]; ++t) s += part[t];
+    out[i] = s * dv[i];
+}
+
+}  // namespace
+}  // namespace phix
+
+using namespace phix;
+
+struct phix_batch {
+    int phys = 0, scheme = 0, prec = 0, ninst = 0, nf = 1;
+    double dt = 0.0;
+    size_t esz = 8;
+    std::vector<phix_grid_t> grids;
+    std::vector<Layout> layouts;
+    std::vector<size_t> stored;
+    std::vector<double> prm;          // ninst x 8
+    void* pool = nullptr;             // all buffers
+    std::vector<void*> st[2], kb[3];  // per instance (field 0 only: batch supports 1-field physics)
+    int cur = 0;
+    int cfg = 0, ctas_per_sm = 0, nsm = 148;
+    // device-side argument tables: [stage kind][parity] -> ninst StageArgs
+    void* args_dev = nullptr;
+    size_t args_bytes = 0;
+    BatchTile* tiles_dev = nullptr;
+    int ntiles = 0, tiles_cfg = -1;
+    int* first_dev = nullptr;         // instance -> first tile index (ninst+1)
+    double* dv_dev = nullptr;
+    double* part_dev = nullptr;
+    double* mass_dev = nullptr;
+    cudaStream_t cap = nullptr;
+    int graph_steps = 0;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+};
+
+namespace phix {
+namespace {
+
+void batch_drop_graphs(phix_batch* b) {
+    for (auto& e : b->gexec)
+        if (e) { cudaGraphExecDestroy(e); e = nullptr; }
+}
+
+// Tile list for tile config `cfg`: instances in descending size, so the
+// persistent CTAs' round-robin walk over the list stays balanced.
+int build_tiles(phix_batch* b, int cfg) {
+    if (b->tiles_cfg == cfg) return PHIX_OK;
+    const TileCfg tc = kTileCfgs[cfg];
+    std::vector<int> order(b->ninst);
+    for (int i = 0; i < b->ninst; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return (long long)b->grids[a].n[0] * b->grids[a].n[1] > (long long)b->grids[c].n[0] * b->grids[c].n[1];
+    });
+    std::vector<BatchTile> tiles;
+    // tiles grouped per instance (for the mass sums) in the size order
+    std::vector<std::vector<BatchTile>> per(b->ninst);
+    for (int i = 0; i < b->ninst; ++i) {
+        const phix_grid_t& g = b->grids[i];
+        for (int y = 0; y < g.n[1]; y += tc.ty)
+            for (int x = 0; x < g.n[0]; x += tc.tx) per[i].push_back({i, x, y, 0});
+    }
+    std::vector<int> pos(b->ninst);
+    for (int oi = 0; oi < b->ninst; ++oi) {
+        const int i = order[oi];
+        pos[i] = (int)tiles.size();
+        tiles.insert(tiles.end(), per[i].begin(), per[i].end());
+    }
+    // instance i's tiles are contiguous at [pos[i], pos[i] + per[i].size())
+    if (b->first_dev) cudaFree(b->first_dev);
+    if (b->tiles_dev) cudaFree(b->tiles_dev);
+    if (b->part_dev) cudaFree(b->part_dev);
+    b->first_dev = nullptr;
+    b->tiles_dev = nullptr;
+    b->part_dev = nullptr;
+    // encode [start, end) per instance as two arrays packed: first[i] = start, first[ninst + 1 + i] = end
+    std::vector<int> se(2 * (b->ninst + 1), 0);
+    for (int i = 0; i < b->ninst; ++i) {
+        se[i] = pos[i];
+        se[b->ninst + 1 + i] = pos[i] + (int)per[i].size();
+    }
+    b->ntiles = (int)tiles.size();
+    PHIX_TRY_CUDA(cudaMalloc(&b->tiles_dev, sizeof(BatchTile) * tiles.size()));
+    PHIX_TRY_CUDA(cudaMemcpy(b->tiles_dev, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice));
+    PHIX_TRY_CUDA(cudaMalloc(&b->first_dev, sizeof(int) * se.size()));
+    PHIX_TRY_CUDA(cudaMemcpy(b->first_dev, se.data(), sizeof(int) * se.size(), cudaMemcpyHostToDevice));
+    PHIX_TRY_CUDA(cudaMalloc(&b->part_dev, sizeof(double) * tiles.size()));
+    b->tiles_cfg = cfg;
+    batch_drop_graphs(b);
+    return PHIX_OK;
+}
+
+template <typename T>
+StageArgs<T>* args_table(phix_batch* b, int kind, int parity) {
+    return reinterpret_cast<StageArgs<T>*>(b->args_dev) + ((size_t)kind * 2 + parity) * b->ninst;
+}
+
+// kinds: 0 = RK4 stage 1, 1 = stage 2, 2 = stage 3, 3 = RK4 final, 4 = Euler final
+template <typename T>
+int build_args(phix_batch* b) {
+    const size_t n = (size_t)5 * 2 * b->ninst;
+    std::vector<StageArgs<T>> h(n);
+    memset(h.data(), 0, sizeof(StageArgs<T>) * n);
+    for (int kind = 0; kind < 5; ++kind)
+        for (int par = 0; par < 2; ++par)
+            for (int i = 0; i < b->ninst; ++i) {
+                StageArgs<T>& A = h[((size_t)kind * 2 + par) * b->ninst + i];
+                const phix_grid_t& g = b->grids[i];
+                A.L = b->layouts[i];
+                for (int a = 0; a < 3; ++a) A.i2[a] = a < g.dim ? (T)(1.0 / (g.d[a] * g.d[a])) : (T)0;
+                make_coeffs<T>(b->phys, &b->prm[8 * i], A.p);
+                A.u[0] = (const T*)b->st[par][i];
+                if (kind == 0) {
+                    A.out[0] = (T*)b->kb[0][i];
+                } else if (kind == 1 || kind == 2) {
+                    A.kin[0] = (const T*)b->kb[kind - 1][i];
+                    A.out[0] = (T*)b->kb[kind][i];
+                    A.a = (T)(b->dt * 0.5);
+                } else if (kind == 3) {
+                    A.kin[0] = (const T*)b->kb[2][i];
+                    A.k1[0] = (const T*)b->kb[0][i];
+                    A.k2[0] = (const T*)b->kb[1][i];
+                    A.out[0] = (T*)b->st[1 - par][i];
+                    A.a = (T)b->dt;
+                    A.dtf = (T)(b->dt / 6.0);
+                } else {
+                    A.out[0] = (T*)b->st[1 - par][i];
+                    A.dtf = (T)b->dt;
+                }
+            }
+    if (!b->args_dev) {
+        b->args_bytes = sizeof(StageArgs<T>) * n;
+        PHIX_TRY_CUDA(cudaMalloc(&b->args_dev, b->args_bytes));
+    }
+    PHIX_TRY_CUDA(cudaMemcpy(b->args_dev, h.data(), sizeof(StageArgs<T>) * n, cudaMemcpyHostToDevice));
+    return PHIX_OK;
+}
+
+template <typename T>
+int batch_step(phix_batch* b, cudaStream_t s) {
+    const int par = b->cur;
+    int rc;
+    if (b->scheme == PHIX_EULER) {
+        rc = launch_batched<T>(b->phys, MODE_EULER_FINAL, b->cfg, args_table<T>(b, 4, par), b->tiles_dev, b->ntiles,
+                               b->ctas_per_sm, b->nsm, s);
+        if (rc) return rc;
+    } else {
+        for (int kind = 0; kind < 3; ++kind)
+            if ((rc = launch_batched<T>(b->phys, MODE_K, b->cfg, args_table<T>(b, kind, par), b->tiles_dev, b->ntiles,
+                                        b->ctas_per_sm, b->nsm, s)))
+                return rc;
+        if ((rc = launch_batched<T>(b->phys, MODE_RK4_FINAL, b->cfg, args_table<T>(b, 3, par), b->tiles_dev,
+                                    b->ntiles, b->ctas_per_sm, b->nsm, s)))
+            return rc;
+    }
+    b->cur = 1 - par;
+    return PHIX_OK;
+}
+
+int batch_steps(phix_batch* b, int n, cudaStream_t s) {
+    for (int i = 0; i < n; ++i) {
+        int rc = b->prec == PHIX_F32 ? batch_step<float>(b, s) : batch_step<double>(b, s);
+        if (rc) return rc;
+    }
+    return PHIX_OK;
+}
+
+int batch_replay(phix_batch* b, cudaStream_t s) {
+    const int parity = b->cur;
+    if (!b->gexec[parity]) {
+        cudaGraph_t graph = nullptr;
+        PHIX_TRY_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+        int rc = batch_steps(b, b->graph_steps, b->cap);
+        cudaError_t e = cudaStreamEndCapture(b->cap, &graph);
+        b->cur = parity;
+        if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+        if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&b->gexec[parity], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+    }
+    PHIX_TRY_CUDA(cudaGraphLaunch(b->gexec[parity], s));
+    count_launch(b->graph_steps * (b->scheme == PHIX_RK4 ? 4 : 1));
+    if (b->graph_steps % 2) b->cur = 1 - parity;
+    return PHIX_OK;
+}
+
+}  // namespace
+}  // namespace phix
+
+extern "C" {
+
+int phix_batch_create(phix_batch_t** out, int phys, int scheme, int precision, int ninst, const phix_grid_t* grids,
+                      const double* prm, double dt) {
+    if (!out || !grids || !prm || ninst < 1) { set_error("batch_create: bad argument"); return PHIX_ERR_ARG; }
+    *out = nullptr;
+    if (phys != PHIX_PHYS_AC && phys != PHIX_PHYS_CH) {
+        set_error("batch: single-field physics only (AC, CH)");
+        return PHIX_ERR_UNSUPPORTED;
+    }
+    if (scheme != PHIX_EULER && scheme != PHIX_RK4) { set_error("batch: unknown scheme %d", scheme); return PHIX_ERR_ARG; }
+    if (precision != PHIX_F32 && precision != PHIX_F64) { set_error("batch: unknown precision"); return PHIX_ERR_ARG; }
+    auto* b = new (std::nothrow) phix_batch();
+    if (!b) { set_error("out of host memory"); return PHIX_ERR_ARG; }
+    b->phys = phys;
+    b->scheme = scheme;
+    b->prec = precision;
+    b->ninst = ninst;
+    b->dt = dt;
+    b->esz = precision == PHIX_F32 ? 4 : 8;
+    b->grids.assign(grids, grids + ninst);
+    b->layouts.resize(ninst);
+    b->stored.resize(ninst);
+    b->prm.assign(prm, prm + 8 * (size_t)ninst);
+    for (int i = 0; i < ninst; ++i) {
+        int rc = validate_grid(&grids[i], &b->layouts[i], &b->stored[i]);
+        if (!rc && grids[i].dim != 2) { set_error("batch: instance %d is not 2-D", i); rc = PHIX_ERR_UNSUPPORTED; }
+        if (rc) { delete b; return rc; }
+    }
+    // pool: per instance 2 states + 3 k (RK4), each padded to 256 bytes
+    const int nbuf = scheme == PHIX_RK4 ? 5 : 2;
+    size_t total = 0;
+    std::vector<size_t> off(ninst);
+    for (int i = 0; i < ninst; ++i) {
+        off[i] = total;
+        total += nbuf * ((b->stored[i] * b->esz + 255) / 256 * 256);
+    }
+    cudaError_t e = cudaMalloc(&b->pool, total);
+    if (e != cudaSuccess) { delete b; return cuda_status(e, "cudaMalloc(batch pool)"); }
+    cudaMemset(b->pool, 0, total);
+    for (int k = 0; k < 2; ++k) b->st[k].resize(ninst);
+    for (int k = 0; k < 3; ++k) b->kb[k].resize(ninst, nullptr);
+    for (int i = 0; i < ninst; ++i) {
+        const size_t sz = (b->stored[i] * b->esz + 255) / 256 * 256;
+        char* base = (char*)b->pool + off[i];
+        b->st[0][i] = base;
+        b->st[1][i] = base + sz;
+        if (scheme == PHIX_RK4)
+            for (int k = 0; k < 3; ++k) b->kb[k][i] = base + (2 + k) * sz;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev);
+    int rc = b->prec == PHIX_F32 ? build_args<float>(b) : build_args<double>(b);
+    if (!rc) rc = build_tiles(b, 0);
+    if (!rc) {
+        std::vector<double> dv(ninst, 1.0);
+        for (int i = 0; i < ninst; ++i)
+            for (int a = 0; a < grids[i].dim; ++a) dv[i] *= grids[i].d[a];
+        e = cudaMalloc(&b->dv_dev, sizeof(double) * ninst);
+        if (e == cudaSuccess) e = cudaMemcpy(b->dv_dev, dv.data(), sizeof(double) * ninst, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc(&b->mass_dev, sizeof(double) * ninst);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+        if (e != cudaSuccess) rc = cuda_status(e, "batch_create");
+    }
+    if (rc) { phix_batch_destroy(b); return rc; }
+    *out = b;
+    return PHIX_OK;
+}
+
+int phix_batch_destroy(phix_batch_t* b) {
+    if (!b) return PHIX_OK;
+    batch_drop_graphs(b);
+    if (b->pool) cudaFree(b->pool);
+    if (b->args_dev) cudaFree(b->args_dev);
+    if (b->tiles_dev) cudaFree(b->tiles_dev);
+    if (b->first_dev) cudaFree(b->first_dev);
+    if (b->part_dev) cudaFree(b->part_dev);
+    if (b->dv_dev) cudaFree(b->dv_dev);
+    if (b->mass_dev) cudaFree(b->mass_dev);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    delete b;
+    return PHIX_OK;
+}
+
+int phix_batch_load(phix_batch_t* b, int inst, const double* field, int from_host, void* stream) {
+    if (!b || !field || inst < 0 || inst >= b->ninst) { set_error("batch_load: bad argument"); return PHIX_ERR_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t S = b->stored[inst];
+    for (int k = 0; k < 2; ++k) {
+        void* dst = b->st[k][inst];
+        if (b->prec == PHIX_F64) {
+            PHIX_TRY_CUDA(cudaMemcpyAsync(dst, field, S * 8, from_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+        } else {
+            if (from_host) {
+                std::vector<float> tmp(S);
+                for (size_t q = 0; q < S; ++q) tmp[q] = (float)field[q];
+                PHIX_TRY_CUDA(cudaMemcpyAsync(dst, tmp.data(), S * 4, cudaMemcpyHostToDevice, s));
+                PHIX_TRY_CUDA(cudaStreamSynchronize(s));
+            } else {
+                int rc = convert_f64_to_f32((float*)dst, field, S, s);
+                if (rc) return rc;
+            }
+        }
+    }
+    return PHIX_OK;
+}
+
+int phix_batch_store(phix_batch_t* b, int inst, double* field, int to_host, void* stream) {
+    if (!b || !field || inst < 0 || inst >= b->ninst) { set_error("batch_store: bad argument"); return PHIX_ERR_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t S = b->stored[inst];
+    const void* src = b->st[b->cur][inst];
+    if (b->prec == PHIX_F64) {
+        PHIX_TRY_CUDA(cudaMemcpyAsync(field, src, S * 8, to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+        if (to_host) PHIX_TRY_CUDA(cudaStreamSynchronize(s));
+        return PHIX_OK;
+    }
+    if (to_host) {
+        std::vector<float> tmp(S);
+        PHIX_TRY_CUDA(cudaMemcpyAsync(tmp.data(), src, S * 4, cudaMemcpyDeviceToHost, s));
+        PHIX_TRY_CUDA(cudaStreamSynchronize(s));
+        for (size_t q = 0; q < S; ++q) field[q] = (double)tmp[q];
+        return PHIX_OK;
+    }
+    return convert_f32_to_f64(field, (const float*)src, S, s);
+}
+
+int phix_batch_set_tiles(phix_batch_t* b, int tile_cfg, int ctas_per_sm) {
+    if (!b || tile_cfg < 0 || tile_cfg >= kNumTileCfgs || ctas_per_sm < 0) {
+        set_error("batch_set_tiles: bad argument");
+        return PHIX_ERR_ARG;
+    }
+    int rc = build_tiles(b, tile_cfg);
+    if (rc) return rc;
+    b->cfg = tile_cfg;
+    b->ctas_per_sm = ctas_per_sm;
+    batch_drop_graphs(b);
+    return PHIX_OK;
+}
+
+int phix_batch_get_tiles(const phix_batch_t* b, int* tile_cfg, int* ctas_per_sm, int* ntiles) {
+    if (!b) { set_error("batch_get_tiles: NULL"); return PHIX_ERR_ARG; }
+    if (tile_cfg) *tile_cfg = b->cfg;
+    if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+    if (ntiles) *ntiles = b->ntiles;
+    return PHIX_OK;
+}
+
+int phix_batch_set_graph(phix_batch_t* b, int steps_per_graph) {
+    if (!b || steps_per_graph < 0) { set_error("batch_set_graph: bad argument"); return PHIX_ERR_ARG; }
+    batch_drop_graphs(b);
+    b->graph_steps = steps_per_graph;
+    return PHIX_OK;
+}
+
+int phix_batch_advance(phix_batch_t* b, int nsteps, void* stream) {
+    if (!b || nsteps < 0) { set_error("batch_advance: bad argument"); return PHIX_ERR_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc;
+    if (b->graph_steps > 0)
+        while (nsteps >= b->graph_steps) {
+            if ((rc = batch_replay(b, s))) return rc;
+            nsteps -= b->graph_steps;
+        }
+    return batch_steps(b, nsteps, s);
+}
+
+int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms) {
+    if (!b || trial_steps < 1) { set_error("batch_autotune: bad argument"); return PHIX_ERR_ARG; }
+    // The state evolves during trials; save and restore it so tuning is invisible.
+    const int cur0 = b->cur;
+    size_t bytes = 0;
+    for (int i = 0; i < b->ninst; ++i) bytes += b->stored[i] * b->esz;
+    void* save = nullptr;
+    PHIX_TRY_CUDA(cudaMalloc(&save, bytes));
+    size_t o = 0;
+    for (int i = 0; i < b->ninst; ++i) {
+        PHIX_TRY_CUDA(cudaMemcpy((char*)save + o, b->st[cur0][i], b->stored[i] * b->esz, cudaMemcpyDeviceToDevice));
+        o += b->stored[i] * b->esz;
+    }
+    const int old_graph = b->graph_steps;
+    b->graph_steps = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    int best_cfg = 0, best_cps = 0;
+    const int cps_options[] = {0, 2, 4};
+    int rc = PHIX_OK;
+    for (int cfg = 0; cfg < kNumTileCfgs && !rc; ++cfg) {
+        for (int cps : cps_options) {
+            if ((rc = phix_batch_set_tiles(b, cfg, cps))) break;
+            if ((rc = batch_steps(b, 1, 0))) break;  // warm-up
+            cudaEventRecord(e0, 0);
+            if ((rc = batch_steps(b, trial_steps, 0))) break;
+            cudaEventRecord(e1, 0);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) { best = ms; best_cfg = cfg; best_cps = cps; }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // restore the state into the buffer that was current
+    b->cur = cur0;
+    o = 0;
+    for (int i = 0; i < b->ninst; ++i) {
+        cudaMemcpy(b->st[cur0][i], (char*)save + o, b->stored[i] * b->esz, cudaMemcpyDeviceToDevice);
+        o += b->stored[i] * b->esz;
+    }
+    cudaFree(save);
+    b->graph_steps = old_graph;
+    if (rc) return rc;
+    rc = phix_batch_set_tiles(b, best_cfg, best_cps);
+    if (best_ms) *best_ms = best / trial_steps;
+    return rc;
+}
+
+int phix_batch_mass(phix_batch_t* b, double* masses) {
+    if (!b || !masses) { set_error("batch_mass: NULL"); return PHIX_ERR_ARG; }
+    const TileCfg tc = kTileCfgs[b->tiles_cfg];
+    const int grid = std::min(b->ntiles, b->nsm * 8);
+    if (b->prec == PHIX_F32)
+        batch_tile_mass<float><<<grid, 256>>>(args_table<float>(b, 0, b->cur), b->tiles_dev, b->ntiles, tc.tx, tc.ty,
+                                              b->part_dev);
+    else
+        batch_tile_mass<double><<<grid, 256>>>(args_table<double>(b, 0, b->cur), b->tiles_dev, b->ntiles, tc.tx,
+                                               tc.ty, b->part_dev);
+    PHIX_LAUNCH_CHECK("batch_tile_mass");
+    batch_inst_sum<<<(b->ninst + 127) / 128, 128>>>(b->part_dev, b->first_dev, b->ninst, b->dv_dev, b->mass_dev);
+    PHIX_LAUNCH_CHECK("batch_inst_sum");
+    PHIX_TRY_CUDA(cudaMemcpy(masses, b->mass_dev, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost));
+    return PHIX_OK;
+}
+
+}  // extern "C"

@@ -49,13 +49,27 @@ static int conv_grid(size_t n) {
     return (int)(b ? b : 1);
 }
 
+int convert_f64_to_f32(float* dst, const double* src, size_t n, cudaStream_t s) {
+    f64_to_f32<<<conv_grid(n), 256, 0, s>>>(dst, src, n, aligned16(dst, src));
+    PHIX_LAUNCH_CHECK("f64_to_f32");
+    return PHIX_OK;
+}
+
+int convert_f32_to_f64(double* dst, const float* src, size_t n, cudaStream_t s) {
+    f32_to_f64<<<conv_grid(n), 256, 0, s>>>(dst, src, n, aligned16(dst, src));
+    PHIX_LAUNCH_CHECK("f32_to_f64");
+    return PHIX_OK;
+}
+
 int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s) {
     const size_t S = stepper_stored(h);
     for (int f = 0; f < stepper_nf(h); ++f) {
         if (!fields[f]) { set_error("load: field %d is NULL", f); return PHIX_ERR_ARG; }
         // both ping-pong buffers get the full stored array, so ghost layers
         // that no BC rewrites stay identical whichever buffer is current
-        for (int b = 0; b < 2; ++b) {
+        // (the multi-step mu has one buffer)
+        const int nb = (stepper_scheme(h) == PHIX_MULTISTEP && f == 1) ? 1 : 2;
+        for (int b = 0; b < nb; ++b) {
             void* dst = stepper_state_buf(h, b, f);
             if (stepper_prec(h) == PHIX_F64) {
                 if (dst == (const void*)fields[f]) continue;
@@ -66,6 +80,7 @@ int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s
             }
         }
     }
+    stepper_mark_mu_zero(h);
     return PHIX_OK;
 }
 
@@ -86,7 +101,7 @@ int stepper_copy_out(phix_stepper* h, double* const* fields, cudaStream_t s) {
 }
 
 int stepper_diag(phix_stepper* h, double* out) {
-    const int nf = stepper_nf(h);
+    const int nf = physics_nfields(stepper_phys(h));
     const int np = reduce_partials_needed(stepper_grid(h));
     double* part = stepper_partials(h, np);
     if (!part) { set_error("diagnostics: cudaMalloc failed"); return PHIX_ERR_CUDA; }

@@ -23,7 +23,11 @@
 
 namespace phix {
 
-enum : int { MODE_K = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2 };
+// MODE_MULTISTEP: the reference's multi-step Euler Cahn-Hilliard
+// (Solver.cu:317-340 with Cahn-Hillard_double-well.cu:84-106): mu (STEADY) is
+// the smem mu of the tile, written out as a field; c (TRANSIENT) gets the
+// Euler update from M*lap(mu).
+enum : int { MODE_K = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2, MODE_MULTISTEP = 3 };
 
 template <typename T>
 struct StageArgs {
@@ -33,6 +37,7 @@ struct StageArgs {
     const T* k1[2];   // RK4 final stage only
     const T* k2[2];
     T* out[2];        // k_s, or the new state in the final modes
+    T* mu_out;        // MODE_MULTISTEP: the STEADY mu field
     T a;              // y = u + a * kin
     T dtf;            // dt/6 (RK4 final) or dt (Euler)
     T i2[3];          // 1/d^2 per axis
@@ -152,7 +157,7 @@ template <typename T, int MODE>
 __device__ __forceinline__ void emit(const StageArgs<T>& A, int f, int idx, T k) {
     if (MODE == MODE_K) {
         A.out[f][idx] = k;
-    } else if (MODE == MODE_EULER_FINAL) {
+    } else if (MODE == MODE_EULER_FINAL || MODE == MODE_MULTISTEP) {
         A.out[f][idx] = rfma(A.dtf, k, __ldg(A.u[f] + idx));
     } else {
         // phi += dt6 * (((k1 + 2 k2) + 2 k3) + k4)
@@ -178,18 +183,27 @@ __device__ __forceinline__ void write_ghost(const StageArgs<T>& A, int nf, int p
 // ---------------------------------------------------------------------------
 // 1-D / 2-D: box tile
 // ---------------------------------------------------------------------------
-template <typename T, int PHYS, int DIM, int MODE, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) stage_box(const StageArgs<T> A) {
+// Shared memory of one box tile.
+template <typename T, int PHYS, int DIM, int TX, int TY>
+struct BoxSmem {
     using P = PhysTraits<PHYS>;
-    constexpr int NF = P::NF, H = P::H;
-    constexpr int HY = DIM >= 2 ? H : 0;
-    constexpr int WX = TX + 2 * H, WY = TY + 2 * HY;
-    constexpr int MX = TX + 2, MY = TY + (DIM >= 2 ? 2 : 0);
-    __shared__ T ys[NF][WY * WX];
-    __shared__ T ms[P::MU ? MY * MX : 1];
+    static constexpr int H = P::H, HY = DIM >= 2 ? P::H : 0;
+    static constexpr int WX = TX + 2 * H, WY = TY + 2 * HY;
+    static constexpr int MX = TX + 2, MY = TY + (DIM >= 2 ? 2 : 0);
+    T ys[P::NF][WY * WX];
+    T ms[P::MU ? MY * MX : 1];
+};
+
+// One TX x TY tile whose first physical cell is (x0, y0).
+template <typename T, int PHYS, int DIM, int MODE, int TX, int TY, int NT>
+__device__ __forceinline__ void box_tile(const StageArgs<T>& A, BoxSmem<T, PHYS, DIM, TX, TY>& sm, int x0, int y0) {
+    using P = PhysTraits<PHYS>;
+    using S = BoxSmem<T, PHYS, DIM, TX, TY>;
+    constexpr int NF = P::NF, H = S::H, HY = S::HY, WX = S::WX, WY = S::WY, MX = S::MX, MY = S::MY;
+    T(&ys)[NF][WY * WX] = sm.ys;
+    T* ms = sm.ms;
 
     const int n0 = A.L.n[0], n1 = A.L.n[1];
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const bool interior = x0 - H >= 0 && x0 + TX + H <= n0 && (DIM < 2 || (y0 - HY >= 0 && y0 + TY + HY <= n1));
 
     for (int i = threadIdx.x; i < WX * WY; i += NT) {
@@ -236,6 +250,22 @@ __global__ void __launch_bounds__(NT) stage_box(const StageArgs<T> A) {
         const int idx = A.L.origin + px + A.L.s[1] * py;
 #pragma unroll
         for (int f = 0; f < NF; ++f) emit<T, MODE>(A, f, idx, k[f]);
+        if (MODE == MODE_MULTISTEP) A.mu_out[idx] = ms[moff];
+    }
+
+    if (MODE == MODE_MULTISTEP && !interior) {
+        // ghost layer 1 of mu: the BC-mapped ring values (the STEADY field is
+        // zeroed, written, then its BCs run before the TRANSIENT step reads it)
+        for (int i = threadIdx.x; i < MX * MY; i += NT) {
+            const int lx = i % MX, ly = i / MX;
+            const int px = x0 - 1 + lx, py = y0 - (DIM >= 2 ? 1 : 0) + ly;
+            const bool outx = px < 0 || px >= n0, outy = DIM >= 2 && (py < 0 || py >= n1);
+            if (outx == outy) continue;  // interior or corner
+            if (outx && (py < y0 || py >= y0 + TY)) continue;  // owned by the neighbour tile row
+            if (outy && (px < x0 || px >= x0 + TX)) continue;
+            if (A.L.bc[(outx ? 0 : 2) + ((outx ? px : py) < 0 ? 0 : 1)] == PHIX_BC_NONE) continue;
+            A.mu_out[A.L.origin + px + A.L.s[1] * py] = ms[i];
+        }
     }
 
     if (MODE != MODE_K && !interior) {
@@ -258,6 +288,31 @@ __global__ void __launch_bounds__(NT) stage_box(const StageArgs<T> A) {
                 if (y0 + TY >= n1) write_ghost<T, DIM>(A, NF, px, n1 - 1 + l, 0);
             }
         }
+    }
+}
+
+// Single field: one CTA per tile.
+template <typename T, int PHYS, int DIM, int MODE, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) stage_box(const StageArgs<T> A) {
+    __shared__ BoxSmem<T, PHYS, DIM, TX, TY> sm;
+    box_tile<T, PHYS, DIM, MODE, TX, TY, NT>(A, sm, blockIdx.x * TX, blockIdx.y * TY);
+}
+
+// Many independent fields in one persistent launch: CTA b walks the tile list
+// b, b + gridDim.x, ...; tile t = (instance, x0, y0) and the instance's stage
+// arguments come from `args` (one StageArgs per instance for this stage).
+struct BatchTile {
+    int inst, x0, y0, pad;
+};
+
+template <typename T, int PHYS, int MODE, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) stage_box_batched(const StageArgs<T>* __restrict__ args,
+                                                        const BatchTile* __restrict__ tiles, int ntiles) {
+    __shared__ BoxSmem<T, PHYS, 2, TX, TY> sm;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const BatchTile bt = tiles[t];
+        box_tile<T, PHYS, 2, MODE, TX, TY, NT>(args[bt.inst], sm, bt.x0, bt.y0);
+        __syncthreads();  // shared memory is reused by the next tile
     }
 }
 

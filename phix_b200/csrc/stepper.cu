@@ -97,6 +97,12 @@ int launch_mode(int dim, int mode, const StageArgs<T>& A, cudaStream_t s) {
         case MODE_K: return launch_dim<T, PHYS, MODE_K>(dim, A, s);
         case MODE_RK4_FINAL: return launch_dim<T, PHYS, MODE_RK4_FINAL>(dim, A, s);
         case MODE_EULER_FINAL: return launch_dim<T, PHYS, MODE_EULER_FINAL>(dim, A, s);
+        case MODE_MULTISTEP:
+            if (PHYS == PHIX_PHYS_CH && dim <= 2) {
+                if (dim == 1) return launch_box<T, PHIX_PHYS_CH, 1, MODE_MULTISTEP>(A, s);
+                return launch_box<T, PHIX_PHYS_CH, 2, MODE_MULTISTEP>(A, s);
+            }
+            break;
     }
     set_error("stage: bad mode %d", mode);
     return PHIX_ERR_ARG;
@@ -211,6 +217,7 @@ struct phix_stepper {
     bool own_state = true;
     void* kbuf[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
     int cur = 0;
+    bool mu_zero_pending = false;  // MULTISTEP: the STEADY field is zeroed by its first evaluation
     cudaStream_t cap = nullptr;
     int graph_steps = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -236,7 +243,14 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
     const int c = h->cur, o = 1 - c;
     for (int f = 0; f < h->nf; ++f) A.u[f] = (const T*)h->st[c][f];
     int rc;
-    if (h->scheme == PHIX_EULER) {
+    if (h->scheme == PHIX_MULTISTEP) {
+        A.u[1] = nullptr;
+        A.out[0] = (T*)h->st[o][0];
+        A.mu_out = (T*)h->st[0][1];
+        A.dtf = (T)h->dt;
+        rc = launch_stage<T>(h->phys, h->dim, MODE_MULTISTEP, A, s);
+        if (rc) return rc;
+    } else if (h->scheme == PHIX_EULER) {
         for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->st[o][f];
         A.dtf = (T)h->dt;
         rc = launch_stage<T>(h->phys, h->dim, MODE_EULER_FINAL, A, s);
@@ -308,19 +322,26 @@ int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precisio
     if (!out) { set_error("out is NULL"); return PHIX_ERR_ARG; }
     *out = nullptr;
     if (physics_nfields(phys) == 0) { set_error("unknown physics %d", phys); return PHIX_ERR_ARG; }
-    if (scheme != PHIX_EULER && scheme != PHIX_RK4) { set_error("unknown scheme %d", scheme); return PHIX_ERR_ARG; }
+    if (scheme != PHIX_EULER && scheme != PHIX_RK4 && scheme != PHIX_MULTISTEP) {
+        set_error("unknown scheme %d", scheme);
+        return PHIX_ERR_ARG;
+    }
     if (precision != PHIX_F32 && precision != PHIX_F64) { set_error("unknown precision %d", precision); return PHIX_ERR_ARG; }
     if (!prm) { set_error("prm is NULL"); return PHIX_ERR_ARG; }
     Layout L;
     size_t S;
     int rc = validate_grid(g, &L, &S);
     if (rc) return rc;
+    if (scheme == PHIX_MULTISTEP && (phys != PHIX_PHYS_CH || g->dim > 2 || g->ghost != 1)) {
+        set_error("multi-step scheme: Cahn-Hilliard on 1-D/2-D grids with ghost 1 only");
+        return PHIX_ERR_UNSUPPORTED;
+    }
     auto* h = new (std::nothrow) phix_stepper();
     if (!h) { set_error("out of host memory"); return PHIX_ERR_ARG; }
     h->phys = phys;
     h->scheme = scheme;
     h->prec = precision;
-    h->nf = physics_nfields(phys);
+    h->nf = scheme == PHIX_MULTISTEP ? 2 : physics_nfields(phys);
     h->dim = g->dim;
     memcpy(h->prm, prm, sizeof(double) * (phys == PHIX_PHYS_AC ? 2 : 5));
     h->dt = dt;
@@ -387,8 +408,13 @@ int phix_stepper_set_graph(phix_stepper_t* h, int steps_per_graph) {
 int phix_stepper_bind(phix_stepper_t* h, double* const* fields, double* const* alt) {
     if (!h || !fields || !alt) { set_error("bind: NULL argument"); return PHIX_ERR_ARG; }
     if (h->prec != PHIX_F64) { set_error("bind: only FP64 steppers run on caller buffers"); return PHIX_ERR_UNSUPPORTED; }
-    for (int f = 0; f < h->nf; ++f)
-        if (!fields[f] || !alt[f] || fields[f] == alt[f]) { set_error("bind: field %d buffers invalid", f); return PHIX_ERR_ARG; }
+    for (int f = 0; f < h->nf; ++f) {
+        const bool single = h->scheme == PHIX_MULTISTEP && f == 1;  // mu: one buffer
+        if (!fields[f] || (!single && (!alt[f] || fields[f] == alt[f]))) {
+            set_error("bind: field %d buffers invalid", f);
+            return PHIX_ERR_ARG;
+        }
+    }
     drop_graphs(h);
     if (h->own_state)
         for (auto& b : h->st)
@@ -397,9 +423,10 @@ int phix_stepper_bind(phix_stepper_t* h, double* const* fields, double* const* a
     h->own_state = false;
     for (int f = 0; f < h->nf; ++f) {
         h->st[0][f] = fields[f];
-        h->st[1][f] = alt[f];
+        h->st[1][f] = alt[f] ? alt[f] : fields[f];
     }
     h->cur = 0;
+    h->mu_zero_pending = h->scheme == PHIX_MULTISTEP;
     return PHIX_OK;
 }
 
@@ -408,6 +435,10 @@ int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream) {
     if (!h->st[0][0]) { set_error("advance: stepper has no state buffers"); return PHIX_ERR_ARG; }
     cudaStream_t s = (cudaStream_t)stream;
     int rc;
+    if (h->mu_zero_pending && nsteps > 0) {
+        PHIX_TRY_CUDA(cudaMemsetAsync(h->st[0][1], 0, h->S * h->esz, s));
+        h->mu_zero_pending = false;
+    }
     if (h->graph_steps > 0) {
         while (nsteps >= h->graph_steps) {
             if ((rc = replay_group(h, s))) return rc;
@@ -424,7 +455,12 @@ namespace phix {
 int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s);
 int stepper_copy_out(phix_stepper* h, double* const* fields, cudaStream_t s);
 int stepper_diag(phix_stepper* h, double* out);
-void* stepper_state(phix_stepper* h, int f) { return h->st[h->cur][f]; }
+void* stepper_state(phix_stepper* h, int f) {
+    if (h->scheme == PHIX_MULTISTEP && f == 1) return h->st[0][1];  // single mu buffer
+    return h->st[h->cur][f];
+}
+int stepper_scheme(const phix_stepper* h) { return h->scheme; }
+void stepper_mark_mu_zero(phix_stepper* h) { h->mu_zero_pending = h->scheme == PHIX_MULTISTEP; }
 void* stepper_state_buf(phix_stepper* h, int b, int f) { return h->st[b][f]; }
 size_t stepper_stored(const phix_stepper* h) { return h->S; }
 int stepper_prec(const phix_stepper* h) { return h->prec; }

@@ -24,10 +24,16 @@ size_t stepper_stored(const phix_stepper* h);
 int stepper_prec(const phix_stepper* h);
 int stepper_nf(const phix_stepper* h);
 int stepper_phys(const phix_stepper* h);
+int stepper_scheme(const phix_stepper* h);
+void stepper_mark_mu_zero(phix_stepper* h);
 const phix_grid_t* stepper_grid(const phix_stepper* h);
 const double* stepper_prm(const phix_stepper* h);
 double* stepper_staging(phix_stepper* h);
 double* stepper_partials(phix_stepper* h, int n);
+
+// FP64 <-> FP32 copies of n stored elements (convert.cu)
+int convert_f64_to_f32(float* dst, const double* src, size_t n, cudaStream_t s);
+int convert_f32_to_f64(double* dst, const float* src, size_t n, cudaStream_t s);
 
 // diagnostics core (reduce.cu): fields in precision T, FP64 accumulation.
 template <typename T>

@@ -47,3 +47,26 @@ def chac3d(n=256, seed=2, nsteps=5000):
     c = 0.4 + rng.uniform(-0.01, 0.01, size=(n, n, n))
     eta = rng.uniform(0.0, 0.1, size=(n, n, n))
     return g, PHYS_CHAC, [1.0, 1.0, 0.5, 0.5, 1.0], RK4, 0.002, nsteps, [_stored(g, c), _stored(g, eta)]
+
+
+BATCH_SIZES = (128, 256, 384, 512, 768, 1024)
+
+
+def ch2d_batch(ninst=64, seed=3, nsteps=5000, dt=0.005, sizes=BATCH_SIZES):
+    """Batched 2-D Cahn-Hilliard: `ninst` independent periodic instances, grid
+    n x n with n drawn uniformly from `sizes`, kappa ~ U[0.25, 2],
+    M ~ U[0.5, 2], mean c ~ U[0.3, 0.7] plus U[-0.01, 0.01] noise, RK4.
+    Draw order per instance: size, kappa, M, mean, noise field."""
+    rng = np.random.default_rng(seed)
+    grids, prms, fields = [], [], []
+    for _ in range(ninst):
+        n = int(rng.choice(sizes))
+        kappa = float(rng.uniform(0.25, 2.0))
+        M = float(rng.uniform(0.5, 2.0))
+        cbar = float(rng.uniform(0.3, 0.7))
+        g = make_grid((n, n))
+        c = cbar + rng.uniform(-0.01, 0.01, size=(1, n, n))
+        grids.append(g)
+        prms.append([M, kappa, 1.0, 0.0, 1.0])
+        fields.append(_stored(g, c))
+    return grids, PHYS_CH, prms, RK4, dt, nsteps, fields
