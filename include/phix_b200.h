@@ -195,6 +195,41 @@ int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms);
 /* FP64 mass (sum of u * dV over physical cells) per instance; synchronous. */
 int phix_batch_mass(phix_batch_t* b, double* masses);
 
+/* ---- learned surrogate (Cahn-Hilliard, 50 FD steps per call) ----------- */
+
+/* A 4-layer 3x3 CNN (1 -> 32 -> 32 -> 32 -> 1, GELU, circular padding) that
+ * predicts c(t + 50 dt) - c(t) from c(t), followed by an exact FP64
+ * mean-mass projection.  The 32 -> 32 layers (forward, data gradient and
+ * weight gradient) run as BF16 implicit GEMMs on the tcgen05 tensor cores
+ * with FP32 accumulation in TMEM.  States are compact [B][H][W] FP64 device
+ * arrays; W must be a multiple of 128.  No reference counterpart: the
+ * reference only has the FD solver (Solver.cu). */
+typedef struct phix_surrogate phix_surrogate_t;
+int phix_surrogate_create(phix_surrogate_t** out, int H, int W, int batch_max, double in_shift, double in_scale,
+                          double out_scale);
+int phix_surrogate_destroy(phix_surrogate_t* s);
+/* Number of FP32 parameters: W1[32][9] b1[32] W2[32][9][32] b2[32]
+ * W3[32][9][32] b3[32] W4[9][32] b4[1], W[n][tap][ci] with tap = 3*ky + kx. */
+int phix_surrogate_nparams(void);
+int phix_surrogate_set_params(phix_surrogate_t* s, const float* host_params);
+int phix_surrogate_get_params(phix_surrogate_t* s, float* host_params, float* host_grads);
+/* c_out = c + out_scale * net(c), then c_out += mean(c) - mean(c_out). */
+int phix_surrogate_step(phix_surrogate_t* s, const double* c, double* c_out, int B, void* stream);
+/* Raw network output o = net(c) as FP32 [B][H][W]. */
+int phix_surrogate_forward(phix_surrogate_t* s, const double* c, float* o, int B, void* stream);
+/* Gradient of mean((o - (c_next - c)/out_scale)^2) into the internal
+ * gradient vector; *loss = the loss.  Synchronous. */
+int phix_surrogate_grad(phix_surrogate_t* s, const double* c, const double* c_next, int B, double* loss,
+                        void* stream);
+/* Adam step (lr) with `grads` (device FP32, NULL = internal vector). */
+int phix_surrogate_adam(phix_surrogate_t* s, const float* grads, float lr, void* stream);
+/* Device pointer of the internal FP32 gradient vector. */
+float* phix_surrogate_grad_ptr(phix_surrogate_t* s);
+/* Copy the physical plane of a 2-D FP64 stored field to / from a compact
+ * [H][W] array. */
+int phix_plane_gather(const double* stored, double* plane, int H, int W, int ghost, void* stream);
+int phix_plane_scatter(const double* plane, double* stored, int H, int W, int ghost, void* stream);
+
 /* ---- diagnostics (FP64 accumulation) ----------------------------------- */
 
 /* out[0] = sum_phys u * dV (mass), out[1] = free energy

@@ -119,6 +119,7 @@ class Oracle:
             getattr(L, "or_advance" + sfx).restype = C.c_int
             getattr(L, "or_advance_ch_multistep" + sfx).argtypes = [P, P, C.POINTER(C.c_double), C.c_double,
                                                                     C.c_int, g]
+            getattr(L, "or_axpy" + sfx).argtypes = [P, P, C.c_double, C.c_long, C.c_int]
             getattr(L, "or_mass" + sfx).argtypes = [P, g]
             getattr(L, "or_mass" + sfx).restype = C.c_double
             getattr(L, "or_energy" + sfx).argtypes = [PP, C.c_int, C.POINTER(C.c_double), g]
@@ -184,6 +185,10 @@ class Oracle:
         gt = grid.ctype(fma_mode)
         p = (C.c_double * 8)(*(list(prm) + [0.0] * (8 - len(prm))))
         getattr(self.lib, "or_advance_ch_multistep" + s)(_ptr(c, ct), _ptr(mu, ct), p, dt, nsteps, C.byref(gt))
+
+    def axpy(self, dst, src, coeff, fma_mode=1):
+        s, ct = self._sfx(dst)
+        getattr(self.lib, "or_axpy" + s)(_ptr(dst, ct), _ptr(src, ct), coeff, dst.size, fma_mode)
 
     def mass(self, a, grid: Grid) -> float:
         s, ct = self._sfx(a)

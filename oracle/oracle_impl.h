@@ -142,6 +142,12 @@ void FN(or_grad_acc)(REAL* rhs, const REAL* src, double coeff, int axis, const o
     }
 }
 
+/* dst[i] = fma(coeff, src[i], dst[i]) over n elements (kernel_axpy,
+ * Solver.cu:30-35, as the contracted device build computes it). */
+void FN(or_axpy)(REAL* dst, const REAL* src, double coeff, long n, int mode) {
+    for (long i = 0; i < n; ++i) dst[i] = FN(madd)(mode, (REAL)coeff, src[i], dst[i]);
+}
+
 /* ---------------------------------------------------------------------------
  * Pointwise functors (the user lambdas of the reference's drivers).
  * ------------------------------------------------------------------------- */

@@ -118,6 +118,19 @@ def lib() -> C.CDLL:
         "phix_batch_get_tiles": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
         "phix_batch_autotune": ([vp, C.c_int, P], C.c_int),
         "phix_batch_mass": ([vp, P], C.c_int),
+        "phix_surrogate_create": ([C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double],
+                                  C.c_int),
+        "phix_surrogate_destroy": ([vp], C.c_int),
+        "phix_surrogate_nparams": ([], C.c_int),
+        "phix_surrogate_set_params": ([vp, vp], C.c_int),
+        "phix_surrogate_get_params": ([vp, vp, vp], C.c_int),
+        "phix_surrogate_step": ([vp, vp, vp, C.c_int, vp], C.c_int),
+        "phix_surrogate_forward": ([vp, vp, vp, C.c_int, vp], C.c_int),
+        "phix_surrogate_grad": ([vp, vp, vp, C.c_int, P, vp], C.c_int),
+        "phix_surrogate_adam": ([vp, vp, C.c_float, vp], C.c_int),
+        "phix_surrogate_grad_ptr": ([vp], C.c_void_p),
+        "phix_plane_gather": ([vp, vp, C.c_int, C.c_int, C.c_int, vp], C.c_int),
+        "phix_plane_scatter": ([vp, vp, C.c_int, C.c_int, C.c_int, vp], C.c_int),
         "phix_stepper_diagnostics": ([vp, P], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -331,6 +344,90 @@ class Batch:
         out = (C.c_double * self.n)()
         check(lib().phix_batch_mass(self.h, out))
         return list(out)
+
+
+class Surrogate:
+    """Owning wrapper of phix_surrogate_t.  States are [B, H, W] float64 CUDA
+    tensors; parameters travel as flat float32 numpy vectors in the order
+    W1[32][9] b1[32] W2[32][9][32] b2[32] W3[32][9][32] b3[32] W4[9][32] b4[1]."""
+
+    def __init__(self, H: int, W: int, batch_max: int, in_shift: float, in_scale: float, out_scale: float):
+        self.H, self.W, self.bmax = H, W, batch_max
+        self.in_shift, self.in_scale, self.out_scale = in_shift, in_scale, out_scale
+        h = C.c_void_p()
+        check(lib().phix_surrogate_create(C.byref(h), H, W, batch_max, in_shift, in_scale, out_scale))
+        self.h = h
+        self.nparams = lib().phix_surrogate_nparams()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().phix_surrogate_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, flat: np.ndarray):
+        flat = np.ascontiguousarray(flat, dtype=np.float32)
+        assert flat.size == self.nparams
+        check(lib().phix_surrogate_set_params(self.h, C.c_void_p(flat.ctypes.data)))
+
+    def get_params(self):
+        p = np.empty(self.nparams, np.float32)
+        g = np.empty(self.nparams, np.float32)
+        check(lib().phix_surrogate_get_params(self.h, C.c_void_p(p.ctypes.data), C.c_void_p(g.ctypes.data)))
+        return p, g
+
+    def step(self, c, c_out, stream=None):
+        check(lib().phix_surrogate_step(self.h, C.c_void_p(c.data_ptr()), C.c_void_p(c_out.data_ptr()),
+                                        c.shape[0], _stream(stream)))
+
+    def forward(self, c, o, stream=None):
+        check(lib().phix_surrogate_forward(self.h, C.c_void_p(c.data_ptr()), C.c_void_p(o.data_ptr()),
+                                           c.shape[0], _stream(stream)))
+
+    def grad(self, c, c_next, stream=None) -> float:
+        loss = C.c_double()
+        check(lib().phix_surrogate_grad(self.h, C.c_void_p(c.data_ptr()), C.c_void_p(c_next.data_ptr()),
+                                        c.shape[0], C.byref(loss), _stream(stream)))
+        return loss.value
+
+    def grad_ptr(self) -> int:
+        return lib().phix_surrogate_grad_ptr(self.h)
+
+    def adam(self, lr: float, grads=None, stream=None):
+        gp = C.c_void_p(grads.data_ptr()) if grads is not None else None
+        check(lib().phix_surrogate_adam(self.h, gp, lr, _stream(stream)))
+
+
+def plane_gather(stored, plane, H: int, W: int, ghost: int = 1, stream=None):
+    check(lib().phix_plane_gather(C.c_void_p(stored.data_ptr()), C.c_void_p(plane.data_ptr()), H, W, ghost,
+                                  _stream(stream)))
+
+
+def plane_scatter(plane, stored, H: int, W: int, ghost: int = 1, stream=None):
+    check(lib().phix_plane_scatter(C.c_void_p(plane.data_ptr()), C.c_void_p(stored.data_ptr()), H, W, ghost,
+                                   _stream(stream)))
+
+
+def surrogate_params_to_flat(params) -> np.ndarray:
+    """Oracle parameter list [W1,b1,...,W4,b4] (W[n,ky,kx,ci]) -> flat vector."""
+    W1, b1, W2, b2, W3, b3, W4, b4 = params
+    parts = [W1.reshape(32, 9), b1, W2.reshape(32, 9, 32), b2, W3.reshape(32, 9, 32), b3, W4.reshape(9, 32), b4]
+    return np.concatenate([np.asarray(p, np.float32).ravel() for p in parts])
+
+
+def surrogate_flat_to_params(flat: np.ndarray):
+    o = 0
+    out = []
+    for shape in ((32, 3, 3, 1), (32,), (32, 3, 3, 32), (32,), (32, 3, 3, 32), (32,), (1, 3, 3, 32), (1,)):
+        n = int(np.prod(shape))
+        out.append(np.asarray(flat[o:o + n], np.float32).reshape(shape))
+        o += n
+    return out
 
 
 def build_library(verbose: bool = False) -> str:

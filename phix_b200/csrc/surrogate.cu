@@ -1,0 +1,859 @@
+// surrogate.cu -- learned Cahn-Hilliard surrogate: a 4-layer 3x3 CNN
+// (1 -> 32 -> 32 -> 32 -> 1, GELU, circular padding) that advances c by 50
+// FD time steps, followed by an exact FP64 mean-mass projection.
+//
+// The two 32 -> 32 layers carry 97% of the FLOPs and run on the 5th-gen
+// tensor cores as implicit GEMMs (tcgen05.mma kind::f16, BF16 operands from
+// shared memory, FP32 accumulator in TMEM):
+//   forward / data-gradient : M = 128 output pixels of one row, N = 32
+//       channels, K = 9 taps x 32 channels = 18 MMAs of K = 16.  The three
+//       input rows are staged once per tile as [chunk][pixel][8] (K-major,
+//       no swizzle); each tap is the same buffer at a shifted start address.
+//       Epilogue: + bias, GELU, BF16 store (forward) or x GELU'(z) (data
+//       gradient, with the weights flipped and transposed).
+//   weight gradient         : per 16-pixel K step, three MMAs (one per dx)
+//       with M = 128 = (4 staged rows x 32 input channels) and N = 32
+//       output channels, both operands MN-major; accumulators stay in TMEM
+//       for all tiles of the CTA, partial sums per CTA are reduced in a fixed
+//       order.
+// The 1 -> 32 and 32 -> 1 layers (3% of the FLOPs), the loss, Adam and the
+// projection run on CUDA cores.  Activations are NHWC BF16 [B][H][W][32].
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "stepper.h"
+#include "tc_sm100.cuh"
+
+namespace phix {
+namespace sg {
+
+constexpr int CH = 32;
+constexpr int TILE = 128;   // output pixels per tile (one row segment)
+constexpr int NT = 128;     // 4 warps: one per TMEM lane quadrant
+constexpr int HALO_PX = TILE + 2;
+constexpr int CHUNK_B = HALO_PX * 16;  // 2080: one 8-channel chunk of a staged row
+constexpr int ROW_B = 4 * CHUNK_B;     // 8320: one staged row, 32 channels
+constexpr int WPK_B = 9 * 2 * 1024;    // packed weights: (tap, k16) blocks of [2][32][8] bf16
+constexpr int DROW_B = 4 * TILE * 16;  // 8192: one un-haloed row (weight-gradient B operand)
+constexpr uint64_t WAIT_NS = 2000000000ull;  // give up on an mbarrier after 2 s
+
+__device__ __forceinline__ float gelu_f(float x) {
+    const float k = 0.7978845608028654f, c = 0.044715f;
+    return 0.5f * x * (1.0f + tanhf(k * (x + c * x * x * x)));
+}
+__device__ __forceinline__ float gelu_grad_f(float x) {
+    const float k = 0.7978845608028654f, c = 0.044715f;
+    const float t = tanhf(k * (x + c * x * x * x));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * k * (1.0f + 3.0f * c * x * x);
+}
+
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+__device__ __forceinline__ void unpack8(uint4 u, float* f) {
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float2 v = __bfloat1622float2(h[i]);
+        f[2 * i] = v.x;
+        f[2 * i + 1] = v.y;
+    }
+}
+
+__device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// Stage `nrows` input rows y-1 .. y-2+nrows, pixels x0-1 .. x0+TILE, as
+// [row][chunk][pixel][8 channels] (16-byte units, circular wrap).
+__device__ __forceinline__ void stage_rows(uint8_t* rows, const __nv_bfloat16* __restrict__ x, int b, int y, int x0,
+                                           int H, int W, int nrows) {
+    const int units = nrows * HALO_PX * 4;
+    for (int u = threadIdx.x; u < units; u += NT) {
+        const int r = u / (HALO_PX * 4), rem = u - r * HALO_PX * 4, i = rem >> 2, j = rem & 3;
+        const int gy = wrap(y + r - 1, H), gx = wrap(x0 - 1 + i, W);
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(x + (((size_t)b * H + gy) * W + gx) * CH) + j);
+        *reinterpret_cast<uint4*>(rows + r * ROW_B + j * CHUNK_B + i * 16) = v;
+    }
+}
+
+struct ConvArgs {
+    const __nv_bfloat16* x;     // [B][H][W][32]
+    const __nv_bfloat16* wpk;   // packed weights (WPK_B bytes)
+    const float* bias;          // [32] (forward)
+    const __nv_bfloat16* zaux;  // data gradient: pre-activation whose GELU' scales the output
+    __nv_bfloat16* out;         // forward: gelu(z); data gradient: dz
+    __nv_bfloat16* zout;        // forward: z (may be null)
+    int B, H, W;
+    int* err;
+};
+
+enum : int { EPI_FWD = 0, EPI_DGRAD = 1 };
+
+template <int EPI>
+__global__ void __launch_bounds__(NT) conv32_tc(const ConvArgs a) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    uint8_t* wbuf = sm;
+    uint8_t* rows = sm + WPK_B;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + WPK_B + 3 * ROW_B);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    for (int u = threadIdx.x; u < WPK_B / 16; u += NT)
+        reinterpret_cast<uint4*>(wbuf)[u] = __ldg(reinterpret_cast<const uint4*>(a.wpk) + u);
+    if (warp == 0) {
+        tc::tmem_alloc(slot, 32);
+        tc::tmem_relinquish();
+    }
+    if (threadIdx.x == 0) tc::mbar_init(bar, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+    const uint32_t idesc = tc::idesc_bf16_f32(128, 32, 0, 0);
+    const uint32_t rows_a = tc::smem_u32(rows), w_a = tc::smem_u32(wbuf);
+
+    const int tpr = a.W / TILE;
+    const int ntiles = a.B * a.H * tpr;
+    uint32_t phase = 0;
+    bool failed = false;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int b = t / (a.H * tpr), rem = t - b * a.H * tpr, y = rem / tpr, x0 = (rem - y * tpr) * TILE;
+        stage_rows(rows, a.x, b, y, x0, a.H, a.W, 3);
+        tc::fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+                for (int kk = 0; kk < 2; ++kk) {
+                    const int ky = tap / 3, kx = tap % 3;
+                    const uint64_t ad = tc::sdesc(rows_a + ky * ROW_B + 2 * kk * CHUNK_B + kx * 16, CHUNK_B, 128);
+                    const uint64_t bd = tc::sdesc(w_a + (tap * 2 + kk) * 1024, 512, 128);
+                    tc::umma_bf16(tmem, ad, bd, idesc, (tap | kk) != 0);
+                }
+            tc::umma_commit(bar);
+        }
+        if (!tc::mbar_wait_bounded(bar, phase, WAIT_NS)) {
+            failed = true;
+            break;
+        }
+        phase ^= 1u;
+        tc::fence_after_sync();
+        float v[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16), v);
+        const int gx = x0 + warp * 32 + lane;
+        const size_t o = (((size_t)b * a.H + y) * a.W + gx) * CH;
+        uint4* dst = reinterpret_cast<uint4*>(a.out + o);
+        if (EPI == EPI_FWD) {
+#pragma unroll
+            for (int n = 0; n < 32; ++n) v[n] += __ldg(a.bias + n);
+            if (a.zout) {
+                uint4* zd = reinterpret_cast<uint4*>(a.zout + o);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    zd[q] = make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
+                                       pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
+            }
+#pragma unroll
+            for (int n = 0; n < 32; ++n) v[n] = gelu_f(v[n]);
+        } else {
+            const uint4* zp = reinterpret_cast<const uint4*>(a.zaux + o);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float zf[8];
+                unpack8(__ldg(zp + q), zf);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) v[8 * q + e] *= gelu_grad_f(zf[e]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            dst[q] = make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
+                                pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
+        tc::fence_before_sync();
+        __syncthreads();
+    }
+    if (failed && threadIdx.x == 0) atomicExch(a.err, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 32);
+}
+
+struct WgradArgs {
+    const __nv_bfloat16* x;   // layer input [B][H][W][32]
+    const __nv_bfloat16* dz;  // gradient w.r.t. the layer's pre-activation
+    float* partial;           // [gridDim.x][32 n][9 taps][32 ci]
+    int B, H, W;
+    int* err;
+};
+
+__global__ void __launch_bounds__(NT) conv32_wgrad_tc(const WgradArgs a) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    uint8_t* rows = sm;                        // 4 staged rows (the 4th only pads M to 128)
+    uint8_t* drow = sm + 4 * ROW_B;            // [chunk][pixel][8] of dz, row y
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 4 * ROW_B + DROW_B);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        tc::tmem_alloc(slot, 128);
+        tc::tmem_relinquish();
+    }
+    if (threadIdx.x == 0) tc::mbar_init(bar, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+    const uint32_t idesc = tc::idesc_bf16_f32(128, 32, 1, 1);
+    const uint32_t rows_a = tc::smem_u32(rows), d_a = tc::smem_u32(drow);
+    const int tpr = a.W / TILE;
+    const int ntiles = a.B * a.H * tpr;
+    uint32_t phase = 0;
+    bool failed = false, any = false;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int b = t / (a.H * tpr), rem = t - b * a.H * tpr, y = rem / tpr, x0 = (rem - y * tpr) * TILE;
+        stage_rows(rows, a.x, b, y, x0, a.H, a.W, 4);
+        for (int u = threadIdx.x; u < TILE * 4; u += NT) {
+            const int i = u >> 2, j = u & 3;
+            const uint4 v =
+                __ldg(reinterpret_cast<const uint4*>(a.dz + (((size_t)b * a.H + y) * a.W + x0 + i) * CH) + j);
+            *reinterpret_cast<uint4*>(drow + j * (TILE * 16) + i * 16) = v;
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int k = 0; k < TILE / 16; ++k)
+#pragma unroll
+                for (int dx = 0; dx < 3; ++dx) {
+                    const uint64_t ad = tc::sdesc(rows_a + (16 * k + dx) * 16, 128, CHUNK_B);
+                    const uint64_t bd = tc::sdesc(d_a + 16 * k * 16, 128, TILE * 16);
+                    tc::umma_bf16(tmem + dx * 32, ad, bd, idesc, (any || k > 0) ? 1u : 0u);
+                }
+            tc::umma_commit(bar);
+        }
+        any = true;
+        if (!tc::mbar_wait_bounded(bar, phase, WAIT_NS)) {
+            failed = true;
+            break;
+        }
+        phase ^= 1u;
+        tc::fence_before_sync();
+        __syncthreads();  // staged rows are overwritten by the next tile
+    }
+    tc::fence_after_sync();
+    float* part = a.partial + (size_t)blockIdx.x * (32 * 9 * 32);
+    if (!failed && warp < 3) {
+        // D_dx row r*32 + ci (r = ky), column n
+        for (int dx = 0; dx < 3; ++dx) {
+            float v[32];
+            if (any) {
+                tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + dx * 32, v);
+            } else {
+#pragma unroll
+                for (int n = 0; n < 32; ++n) v[n] = 0.f;
+            }
+            const int tap = warp * 3 + dx;
+#pragma unroll
+            for (int n = 0; n < 32; ++n) part[(n * 9 + tap) * 32 + lane] = v[n];
+        }
+    }
+    if (failed && threadIdx.x == 0) atomicExch(a.err, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 128);
+}
+
+// out[i] = sum_b partial[b][i] in block order (deterministic); i < n.
+__global__ void reduce_partials(const float* __restrict__ partial, int nblocks, int n, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float s = 0.f;
+    for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * n + i];
+    out[i] = s;
+}
+
+// ---------------------------------------------------------------------------
+// CUDA-core layers
+// ---------------------------------------------------------------------------
+struct NetParams {
+    double in_shift, in_scale, out_scale;
+};
+
+__device__ __forceinline__ float x0_at(const double* c, int b, int y, int x, int H, int W, NetParams P) {
+    const double v = (c[((size_t)b * H + y) * W + x] - P.in_shift) * P.in_scale;
+    return __bfloat162float(__float2bfloat16_rn((float)v));
+}
+
+// Layer 1: 1 -> 32.  w1 [32 n][9 taps] (bf16-rounded floats), b1 [32].
+__global__ void __launch_bounds__(256) layer1_fwd(const double* __restrict__ c, const float* __restrict__ w1,
+                                                  const float* __restrict__ b1, __nv_bfloat16* __restrict__ z1,
+                                                  __nv_bfloat16* __restrict__ h1, int B, int H, int W, NetParams P) {
+    __shared__ float ws[32 * 9], bs[32];
+    for (int i = threadIdx.x; i < 32 * 9; i += 256) ws[i] = w1[i];
+    if (threadIdx.x < 32) bs[threadIdx.x] = b1[threadIdx.x];
+    __syncthreads();
+    const size_t N = (size_t)B * H * W;
+    for (size_t p = blockIdx.x * 256ull + threadIdx.x; p < N; p += (size_t)gridDim.x * 256) {
+        const int b = (int)(p / ((size_t)H * W)), y = (int)((p / W) % H), x = (int)(p % W);
+        float xv[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) xv[t] = x0_at(c, b, wrap(y + t / 3 - 1, H), wrap(x + t % 3 - 1, W), H, W, P);
+        uint4* zd = reinterpret_cast<uint4*>(z1 + p * CH);
+        uint4* hd = reinterpret_cast<uint4*>(h1 + p * CH);
+        for (int q = 0; q < 4; ++q) {  // one 8-channel group at a time
+            float z[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int n = 8 * q + e;
+                float s = 0.f;
+#pragma unroll
+                for (int t = 0; t < 9; ++t) s = fmaf(xv[t], ws[n * 9 + t], s);
+                z[e] = s + bs[n];
+            }
+            zd[q] = make_uint4(pack2(z[0], z[1]), pack2(z[2], z[3]), pack2(z[4], z[5]), pack2(z[6], z[7]));
+            hd[q] = make_uint4(pack2(gelu_f(z[0]), gelu_f(z[1])), pack2(gelu_f(z[2]), gelu_f(z[3])),
+                               pack2(gelu_f(z[4]), gelu_f(z[5])), pack2(gelu_f(z[6]), gelu_f(z[7])));
+        }
+    }
+}
+
+// Layer 4: 32 -> 1 and the state update  c_out = c + out_scale * o.
+// w4 [9 taps][32 ci], b4 [1].  Per-block FP64 partial sums of c and c_out per
+// image go to part[(blockIdx, image)] for the mean-mass projection; o is also
+// written when `o_out` is non-null (training).
+__global__ void __launch_bounds__(256) layer4_fwd(const __nv_bfloat16* __restrict__ h3, const float* __restrict__ w4,
+                                                  const float* __restrict__ b4, const double* __restrict__ c,
+                                                  double* __restrict__ c_out, float* __restrict__ o_out, int B, int H,
+                                                  int W, NetParams P) {
+    __shared__ float ws[9 * 32];
+    for (int i = threadIdx.x; i < 9 * 32; i += 256) ws[i] = w4[i];
+    __syncthreads();
+    const size_t N = (size_t)B * H * W;
+    for (size_t p = blockIdx.x * 256ull + threadIdx.x; p < N; p += (size_t)gridDim.x * 256) {
+        const int b = (int)(p / ((size_t)H * W)), y = (int)((p / W) % H), x = (int)(p % W);
+        float s = 0.f;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            const size_t q = (((size_t)b * H + wrap(y + t / 3 - 1, H)) * W + wrap(x + t % 3 - 1, W)) * CH;
+            const uint4* src = reinterpret_cast<const uint4*>(h3 + q);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                float f[8];
+                unpack8(__ldg(src + k), f);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) s = fmaf(f[e], ws[t * 32 + 8 * k + e], s);
+            }
+        }
+        const float o = s + b4[0];
+        if (o_out) o_out[p] = o;
+        if (c_out) c_out[p] = c[p] + P.out_scale * (double)o;
+    }
+}
+
+// Per-image FP64 sums of a and b (grid-stride per image: one block row per image).
+__global__ void __launch_bounds__(256) image_sums(const double* __restrict__ a, const double* __restrict__ bb,
+                                                  size_t npix, double* __restrict__ out) {
+    const int img = blockIdx.y;
+    double sa = 0.0, sb = 0.0;
+    for (size_t p = blockIdx.x * 256ull + threadIdx.x; p < npix; p += (size_t)gridDim.x * 256) {
+        sa += a[img * npix + p];
+        sb += bb[img * npix + p];
+    }
+    __shared__ double sh[2][8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sa += __shfl_xor_sync(0xffffffffu, sa, o);
+        sb += __shfl_xor_sync(0xffffffffu, sb, o);
+    }
+    if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = sa; sh[1][threadIdx.x >> 5] = sb; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ta = 0.0, tb = 0.0;
+        for (int w = 0; w < 8; ++w) { ta += sh[0][w]; tb += sh[1][w]; }
+        out[2 * ((size_t)img * gridDim.x + blockIdx.x) + 0] = ta;
+        out[2 * ((size_t)img * gridDim.x + blockIdx.x) + 1] = tb;
+    }
+}
+
+// c_out += (sum(c) - sum(c_out)) / npix per image: the mean-mass projection.
+__global__ void __launch_bounds__(256) project_mass(double* __restrict__ c_out, const double* __restrict__ sums,
+                                                    int nparts, size_t npix) {
+    const int img = blockIdx.y;
+    double sa = 0.0, sb = 0.0;
+    for (int k = 0; k < nparts; ++k) {
+        sa += sums[2 * ((size_t)img * nparts + k)];
+        sb += sums[2 * ((size_t)img * nparts + k) + 1];
+    }
+    const double corr = (sa - sb) / (double)npix;
+    for (size_t p = blockIdx.x * 256ull + threadIdx.x; p < npix; p += (size_t)gridDim.x * 256)
+        c_out[img * npix + p] += corr;
+}
+
+// ---------------------------------------------------------------------------
+// training kernels (CUDA cores)
+// ---------------------------------------------------------------------------
+// do = 2 (o - t) / N with t = (c_next - c) / out_scale; loss partials per block.
+__global__ void __launch_bounds__(256) loss_grad(const float* __restrict__ o, const double* __restrict__ c,
+                                                 const double* __restrict__ cn, float* __restrict__ dO, size_t N,
+                                                 NetParams P, double* __restrict__ lpart) {
+    double s = 0.0;
+    for (size_t p = blockIdx.x * 256ull + threadIdx.x; p < N; p += (size_t)gridDim.x * 256) {
+        const double t = (cn[p] - c[p]) / P.out_scale;
+        const double d = (double)o[p] - t;
+        dO[p] = (float)(2.0 * d / (double)N);
+        s += d * d;
+    }
+    __shared__ double sh[8];
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += sh[w];
+        lpart[blockIdx.x] = t;
+    }
+}
+
+// Layer 4 backward: dz3[p][ci] = (sum_tap dO[p - tap] w4[tap][ci]) * gelu'(z3[p][ci]).
+__global__ void __launch_bounds__(256) layer4_dgrad(const float* __restrict__ dO, const float* __restrict__ w4,
+                                                    const __nv_bfloat16* __restrict__ z3, __nv_bfloat16* __restrict__ dz3,
+                                                    int B, int H, int W) {
+    __shared__ float ws[9 * 32];
+    for (int i = threadIdx.x; i < 9 * 32; i += 256) ws[i] = w4[i];
+    __syncthreads();
+    const size_t N = (size_t)B * H * W;
+    for (size_t p = blockIdx.x * 256ull + threadIdx.x; p < N; p += (size_t)gridDim.x * 256) {
+        const int b = (int)(p / ((size_t)H * W)), y = (int)((p / W) % H), x = (int)(p % W);
+        float d[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t)
+            d[t] = dO[((size_t)b * H + wrap(y - (t / 3 - 1), H)) * W + wrap(x - (t % 3 - 1), W)];
+        const uint4* zp = reinterpret_cast<const uint4*>(z3 + p * CH);
+        uint4* out = reinterpret_cast<uint4*>(dz3 + p * CH);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float zf[8], g[8];
+            unpack8(__ldg(zp + q), zf);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                float s = 0.f;
+#pragma unroll
+                for (int t = 0; t < 9; ++t) s = fmaf(d[t], ws[t * 32 + 8 * q + e], s);
+                g[e] = s * gelu_grad_f(zf[e]);
+            }
+            out[q] = make_uint4(pack2(g[0], g[1]), pack2(g[2], g[3]), pack2(g[4], g[5]), pack2(g[6], g[7]));
+        }
+    }
+}
+
+// Weight gradient of a thin layer on CUDA cores, one partial per block:
+//   mode 4: dw4[tap][ci] = sum_p dO[p] h3[p + tap][ci],  db4 = sum_p dO[p]
+//   mode 1: dw1[n][tap]  = sum_p dz1[p][n] x0[p + tap], db1[n] = sum_p dz1[p][n]
+// Thread j < 288 owns one weight; threads 288..319 own bias terms.
+// The block walks row segments of TILE pixels.
+__global__ void __launch_bounds__(320) thin_wgrad(int mode, const float* __restrict__ dO,
+                                                  const __nv_bfloat16* __restrict__ act, const double* __restrict__ c,
+                                                  int B, int H, int W, NetParams P, float* __restrict__ partial) {
+    __shared__ float dsh[TILE * 32];      // mode 4: dO of the segment; mode 1: dz1[px][n]
+    __shared__ float xsh[3][TILE + 2][1];  // mode 1: x0 rows
+    const int j = threadIdx.x;
+    float acc = 0.f;
+    const int tpr = W / TILE;
+    const int ntiles = B * H * tpr;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int b = t / (H * tpr), rem = t - b * H * tpr, y = rem / tpr, x0 = (rem - y * tpr) * TILE;
+        const size_t base = ((size_t)b * H + y) * W + x0;
+        __syncthreads();
+        if (mode == 4) {
+            for (int i = j; i < TILE; i += 320) dsh[i] = dO[base + i];
+        } else {
+            for (int i = j; i < TILE * 32; i += 320) dsh[i] = __bfloat162float(act[(base + i / 32) * CH + i % 32]);
+            for (int i = j; i < 3 * (TILE + 2); i += 320) {
+                const int r = i / (TILE + 2), k = i % (TILE + 2);
+                xsh[r][k][0] = x0_at(c, b, wrap(y + r - 1, H), wrap(x0 - 1 + k, W), H, W, P);
+            }
+        }
+        __syncthreads();
+        if (mode == 4) {
+            if (j < 288) {
+                const int tap = j / 32, ci = j % 32, ky = tap / 3 - 1, kx = tap % 3 - 1;
+                const size_t row = ((size_t)b * H + wrap(y + ky, H)) * W;
+                for (int i = 0; i < TILE; ++i)
+                    acc = fmaf(dsh[i], __bfloat162float(act[(row + wrap(x0 + i + kx, W)) * CH + ci]), acc);
+            } else if (j == 288) {
+                for (int i = 0; i < TILE; ++i) acc += dsh[i];
+            }
+        } else {
+            if (j < 288) {
+                const int n = j / 9, tap = j % 9, ky = tap / 3, kx = tap % 3;
+                for (int i = 0; i < TILE; ++i) acc = fmaf(dsh[i * 32 + n], xsh[ky][i + kx][0], acc);
+            } else {
+                const int n = j - 288;
+                for (int i = 0; i < TILE; ++i) acc += dsh[i * 32 + n];
+            }
+        }
+    }
+    partial[(size_t)blockIdx.x * 320 + j] = acc;
+}
+
+// Column sums of dz [N][32] -> per-block partial [32] (bias gradient).
+__global__ void __launch_bounds__(256) bias_grad(const __nv_bfloat16* __restrict__ dz, size_t N,
+                                                 float* __restrict__ partial) {
+    __shared__ float sh[8][32];
+    const int c = threadIdx.x & 31, r = threadIdx.x >> 5;
+    float s = 0.f;
+    for (size_t p = blockIdx.x * 8ull + r; p < N; p += (size_t)gridDim.x * 8) s += __bfloat162float(dz[p * CH + c]);
+    sh[r][c] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        float t = 0.f;
+        for (int k = 0; k < 8; ++k) t += sh[k][threadIdx.x];
+        partial[(size_t)blockIdx.x * 32 + threadIdx.x] = t;
+    }
+}
+
+// Adam on the flat FP32 parameter vector (bias-corrected).
+__global__ void adam_step(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// Rebuild the BF16 operands from the FP32 master parameters:
+//   layers 2, 3 forward pack  [tap][k16][chunk][n][8]       = W[n][tap][16k16 + 8chunk + e]
+//   layers 2, 3 dgrad pack    [tap'][k16][chunk][ci][8]     = W[16k16 + 8chunk + e][8 - tap'][ci]
+//   layer 1 / 4 bf16-rounded float copies.
+__global__ void pack_weights(const float* __restrict__ W2, const float* __restrict__ W3, const float* __restrict__ W1,
+                             const float* __restrict__ W4, __nv_bfloat16* __restrict__ pk, float* __restrict__ w1r,
+                             float* __restrict__ w4r) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int P = 9 * 2 * 2 * 32 * 8;  // 9216 elements per pack
+    if (i < 4 * P) {
+        const int which = i / P, r = i % P;
+        const int e = r % 8, row = (r / 8) % 32, chunk = (r / 256) % 2, kk = (r / 512) % 2, tap = r / 1024;
+        const float* Wl = (which & 1) ? W3 : W2;
+        float v;
+        if (which < 2) {  // forward: row = n, k = (tap, ci)
+            const int ci = 16 * kk + 8 * chunk + e;
+            v = Wl[((size_t)row * 9 + tap) * 32 + ci];
+        } else {          // dgrad: row = ci, k = (tap', n)
+            const int n = 16 * kk + 8 * chunk + e;
+            v = Wl[((size_t)n * 9 + (8 - tap)) * 32 + row];
+        }
+        pk[i] = __float2bfloat16_rn(v);
+    } else if (i < 4 * P + 288) {
+        const int k = i - 4 * P;
+        w1r[k] = __bfloat162float(__float2bfloat16_rn(W1[k]));
+    } else if (i < 4 * P + 576) {
+        const int k = i - 4 * P - 288;
+        w4r[k] = __bfloat162float(__float2bfloat16_rn(W4[k]));
+    }
+}
+
+// Extract the compact [H][W] FP64 plane of a 2-D stored field (ghost g).
+__global__ void gather_plane(const double* __restrict__ stored, double* __restrict__ out, int H, int W, int g) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const int sx = W + 2 * g, sy = H + 2 * g;
+    out[(size_t)y * W + x] = stored[(size_t)g * sx * sy + (size_t)(y + g) * sx + (x + g)];
+}
+__global__ void scatter_plane(const double* __restrict__ in, double* __restrict__ stored, int H, int W, int g) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const int sx = W + 2 * g, sy = H + 2 * g;
+    stored[(size_t)g * sx * sy + (size_t)(y + g) * sx + (x + g)] = in[(size_t)y * W + x];
+}
+
+}  // namespace sg
+}  // namespace phix
+
+using namespace phix;
+using namespace phix::sg;
+
+// Parameter vector layout (FP32): W1[32][9] b1[32] W2[32][9][32] b2[32] W3[32][9][32] b3[32] W4[9][32] b4[1]
+// with W[n][ky][kx][ci] flattened (ky, kx) -> tap.
+namespace {
+constexpr int OFF_W1 = 0, OFF_B1 = 288, OFF_W2 = 320, OFF_B2 = 320 + 9216, OFF_W3 = OFF_B2 + 32,
+              OFF_B3 = OFF_W3 + 9216, OFF_W4 = OFF_B3 + 32, OFF_B4 = OFF_W4 + 288, NPARAM = OFF_B4 + 1;
+}
+
+struct phix_surrogate {
+    int H = 0, W = 0, bmax = 0, nsm = 148;
+    NetParams P{};
+    float* params = nullptr;  // NPARAM master FP32
+    float* grads = nullptr;
+    float* adam_m = nullptr;
+    float* adam_v = nullptr;
+    int adam_t = 0;
+    __nv_bfloat16* pk = nullptr;  // 4 packs
+    float* w1r = nullptr;
+    float* w4r = nullptr;
+    __nv_bfloat16 *z1 = nullptr, *h1 = nullptr, *z2 = nullptr, *h2 = nullptr, *z3 = nullptr, *h3 = nullptr;
+    __nv_bfloat16 *dz = nullptr, *dz2 = nullptr;  // gradient scratch
+    float* o = nullptr;
+    float* dO = nullptr;
+    double* sums = nullptr;
+    float* partial = nullptr;  // weight-gradient partials
+    float* thin_out = nullptr; // reduced gradients of the thin layers (320)
+    double* lpart = nullptr;
+    int* err = nullptr;
+    bool packed = false;
+};
+
+namespace {
+
+int sg_conv_grid(const phix_surrogate* s, int B) {
+    const int ntiles = B * s->H * (s->W / TILE);
+    const int g = s->nsm * 4;
+    return ntiles < g ? ntiles : g;
+}
+
+int sg_pack(phix_surrogate* s, cudaStream_t st) {
+    const int total = 4 * 9216 + 576;
+    pack_weights<<<(total + 255) / 256, 256, 0, st>>>(s->params + OFF_W2, s->params + OFF_W3, s->params + OFF_W1,
+                                                      s->params + OFF_W4, s->pk, s->w1r, s->w4r);
+    PHIX_LAUNCH_CHECK("pack_weights");
+    s->packed = true;
+    return PHIX_OK;
+}
+
+int sg_forward(phix_surrogate* s, const double* c, int B, double* c_out, float* o_out, cudaStream_t st) {
+    int rc;
+    if (!s->packed && (rc = sg_pack(s, st))) return rc;
+    const size_t N = (size_t)B * s->H * s->W;
+    const int eg = (int)((N + 255) / 256 < (size_t)s->nsm * 8 ? (N + 255) / 256 : (size_t)s->nsm * 8);
+    layer1_fwd<<<eg, 256, 0, st>>>(c, s->w1r, s->params + OFF_B1, s->z1, s->h1, B, s->H, s->W, s->P);
+    PHIX_LAUNCH_CHECK("layer1_fwd");
+    const size_t smem = WPK_B + 3 * ROW_B + 16;
+    const int cg = sg_conv_grid(s, B);
+    ConvArgs a{};
+    a.B = B; a.H = s->H; a.W = s->W; a.err = s->err;
+    a.x = s->h1; a.wpk = s->pk; a.bias = s->params + OFF_B2; a.out = s->h2; a.zout = s->z2;
+    conv32_tc<EPI_FWD><<<cg, NT, smem, st>>>(a);
+    PHIX_LAUNCH_CHECK("conv32_tc<fwd>");
+    a.x = s->h2; a.wpk = s->pk + 9216; a.bias = s->params + OFF_B3; a.out = s->h3; a.zout = s->z3;
+    conv32_tc<EPI_FWD><<<cg, NT, smem, st>>>(a);
+    PHIX_LAUNCH_CHECK("conv32_tc<fwd>");
+    layer4_fwd<<<eg, 256, 0, st>>>(s->h3, s->w4r, s->params + OFF_B4, c, c_out, o_out, B, s->H, s->W, s->P);
+    PHIX_LAUNCH_CHECK("layer4_fwd");
+    if (c_out) {
+        const size_t npix = (size_t)s->H * s->W;
+        dim3 g(64, B);
+        image_sums<<<g, 256, 0, st>>>(c, c_out, npix, s->sums);
+        PHIX_LAUNCH_CHECK("image_sums");
+        project_mass<<<g, 256, 0, st>>>(c_out, s->sums, 64, npix);
+        PHIX_LAUNCH_CHECK("project_mass");
+    }
+    return PHIX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int phix_surrogate_create(phix_surrogate_t** out, int H, int W, int batch_max, double in_shift, double in_scale,
+                          double out_scale) {
+    if (!out || H < 3 || W < TILE || W % TILE != 0 || batch_max < 1) {
+        set_error("surrogate_create: need H >= 3, W a multiple of %d, batch_max >= 1", TILE);
+        return PHIX_ERR_ARG;
+    }
+    *out = nullptr;
+    auto* s = new (std::nothrow) phix_surrogate();
+    if (!s) { set_error("out of host memory"); return PHIX_ERR_ARG; }
+    s->H = H; s->W = W; s->bmax = batch_max;
+    s->P.in_shift = in_shift; s->P.in_scale = in_scale; s->P.out_scale = out_scale;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, dev);
+    const size_t N = (size_t)batch_max * H * W;
+    const int cgmax = s->nsm * 4;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
+    A((void**)&s->params, NPARAM * 4); A((void**)&s->grads, NPARAM * 4);
+    A((void**)&s->adam_m, NPARAM * 4); A((void**)&s->adam_v, NPARAM * 4);
+    A((void**)&s->pk, 4 * 9216 * 2); A((void**)&s->w1r, 288 * 4); A((void**)&s->w4r, 288 * 4);
+    for (auto** p : {&s->z1, &s->h1, &s->z2, &s->h2, &s->z3, &s->h3, &s->dz, &s->dz2}) A((void**)p, N * CH * 2);
+    A((void**)&s->o, N * 4); A((void**)&s->dO, N * 4);
+    A((void**)&s->sums, sizeof(double) * 2 * 64 * batch_max);
+    A((void**)&s->partial, sizeof(float) * (size_t)cgmax * 9216 + sizeof(float) * 320 * cgmax);
+    A((void**)&s->lpart, sizeof(double) * s->nsm * 8);
+    A((void**)&s->thin_out, sizeof(float) * 320);
+    A((void**)&s->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(s->err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(s->params, 0, NPARAM * 4);
+    if (e == cudaSuccess) e = cudaMemset(s->adam_m, 0, NPARAM * 4);
+    if (e == cudaSuccess) e = cudaMemset(s->adam_v, 0, NPARAM * 4);
+    if (e != cudaSuccess) {
+        int rc = cuda_status(e, "surrogate_create");
+        phix_surrogate_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return PHIX_OK;
+}
+
+int phix_surrogate_destroy(phix_surrogate_t* s) {
+    if (!s) return PHIX_OK;
+    for (void* p : {(void*)s->params, (void*)s->grads, (void*)s->adam_m, (void*)s->adam_v, (void*)s->pk,
+                    (void*)s->w1r, (void*)s->w4r, (void*)s->z1, (void*)s->h1, (void*)s->z2, (void*)s->h2,
+                    (void*)s->z3, (void*)s->h3, (void*)s->dz, (void*)s->dz2, (void*)s->o, (void*)s->dO,
+                    (void*)s->sums, (void*)s->partial, (void*)s->lpart, (void*)s->err, (void*)s->thin_out})
+        if (p) cudaFree(p);
+    delete s;
+    return PHIX_OK;
+}
+
+int phix_surrogate_nparams(void) { return NPARAM; }
+
+int phix_surrogate_set_params(phix_surrogate_t* s, const float* host_params) {
+    if (!s || !host_params) { set_error("set_params: NULL"); return PHIX_ERR_ARG; }
+    PHIX_TRY_CUDA(cudaMemcpy(s->params, host_params, NPARAM * 4, cudaMemcpyHostToDevice));
+    s->packed = false;
+    s->adam_t = 0;
+    PHIX_TRY_CUDA(cudaMemset(s->adam_m, 0, NPARAM * 4));
+    PHIX_TRY_CUDA(cudaMemset(s->adam_v, 0, NPARAM * 4));
+    return PHIX_OK;
+}
+
+int phix_surrogate_get_params(phix_surrogate_t* s, float* host_params, float* host_grads) {
+    if (!s) { set_error("get_params: NULL"); return PHIX_ERR_ARG; }
+    if (host_params) PHIX_TRY_CUDA(cudaMemcpy(host_params, s->params, NPARAM * 4, cudaMemcpyDeviceToHost));
+    if (host_grads) PHIX_TRY_CUDA(cudaMemcpy(host_grads, s->grads, NPARAM * 4, cudaMemcpyDeviceToHost));
+    return PHIX_OK;
+}
+
+// c_out = projection(c + out_scale * net(c)); c, c_out: [B][H][W] FP64 device.
+int phix_surrogate_step(phix_surrogate_t* s, const double* c, double* c_out, int B, void* stream) {
+    if (!s || !c || !c_out || B < 1 || B > s->bmax) { set_error("surrogate_step: bad argument"); return PHIX_ERR_ARG; }
+    return sg_forward(s, c, B, c_out, nullptr, (cudaStream_t)stream);
+}
+
+// Network output o (no update) for tests: o [B][H][W] FP32 device; also leaves
+// the activations of this batch in the internal buffers.
+int phix_surrogate_forward(phix_surrogate_t* s, const double* c, float* o, int B, void* stream) {
+    if (!s || !c || !o || B < 1 || B > s->bmax) { set_error("surrogate_forward: bad argument"); return PHIX_ERR_ARG; }
+    return sg_forward(s, c, B, nullptr, o, (cudaStream_t)stream);
+}
+
+// Gradients of the MSE loss mean((o - (c_next - c)/out_scale)^2) into the
+// internal gradient vector; *loss receives the loss (synchronous).
+int phix_surrogate_grad(phix_surrogate_t* s, const double* c, const double* c_next, int B, double* loss,
+                        void* stream) {
+    if (!s || !c || !c_next || B < 1 || B > s->bmax) { set_error("surrogate_grad: bad argument"); return PHIX_ERR_ARG; }
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = sg_forward(s, c, B, nullptr, s->o, st);
+    if (rc) return rc;
+    const size_t N = (size_t)B * s->H * s->W;
+    const int eg = (int)((N + 255) / 256 < (size_t)s->nsm * 8 ? (N + 255) / 256 : (size_t)s->nsm * 8);
+    loss_grad<<<eg, 256, 0, st>>>(s->o, c, c_next, s->dO, N, s->P, s->lpart);
+    PHIX_LAUNCH_CHECK("loss_grad");
+    const int cg = sg_conv_grid(s, B);
+    const size_t smem_c = WPK_B + 3 * ROW_B + 16, smem_w = 4 * ROW_B + DROW_B + 16;
+    float* part_w = s->partial;                      // cg x 9216
+    float* part_t = s->partial + (size_t)cg * 9216;  // cg x 320
+    // layer 4
+    thin_wgrad<<<cg, 320, 0, st>>>(4, s->dO, s->h3, c, B, s->H, s->W, s->P, part_t);
+    PHIX_LAUNCH_CHECK("thin_wgrad(4)");
+    float* t4 = s->thin_out;  // 288 weights, then the bias at 288
+    reduce_partials<<<2, 256, 0, st>>>(part_t, cg, 320, t4);
+    PHIX_LAUNCH_CHECK("reduce_partials");
+    PHIX_TRY_CUDA(cudaMemcpyAsync(s->grads + OFF_W4, t4, 288 * 4, cudaMemcpyDeviceToDevice, st));
+    PHIX_TRY_CUDA(cudaMemcpyAsync(s->grads + OFF_B4, t4 + 288, 4, cudaMemcpyDeviceToDevice, st));
+    layer4_dgrad<<<eg, 256, 0, st>>>(s->dO, s->w4r, s->z3, s->dz, B, s->H, s->W);
+    PHIX_LAUNCH_CHECK("layer4_dgrad");
+    // layers 3 and 2: weight gradient, bias gradient, data gradient
+    const __nv_bfloat16* acts_in[2] = {s->h2, s->h1};
+    const __nv_bfloat16* zprev[2] = {s->z2, s->z1};
+    const int offW[2] = {OFF_W3, OFF_W2}, offB[2] = {OFF_B3, OFF_B2};
+    const __nv_bfloat16* dpk[2] = {s->pk + 3 * 9216, s->pk + 2 * 9216};
+    __nv_bfloat16* dz_in = s->dz;
+    __nv_bfloat16* dz_out = s->dz2;
+    for (int l = 0; l < 2; ++l) {
+        WgradArgs w{};
+        w.x = acts_in[l]; w.dz = dz_in; w.partial = part_w; w.B = B; w.H = s->H; w.W = s->W; w.err = s->err;
+        conv32_wgrad_tc<<<cg, NT, smem_w, st>>>(w);
+        PHIX_LAUNCH_CHECK("conv32_wgrad_tc");
+        reduce_partials<<<(9216 + 255) / 256, 256, 0, st>>>(part_w, cg, 9216, s->grads + offW[l]);
+        PHIX_LAUNCH_CHECK("reduce_partials");
+        bias_grad<<<cg, 256, 0, st>>>(dz_in, N, part_t);
+        PHIX_LAUNCH_CHECK("bias_grad");
+        reduce_partials<<<1, 32, 0, st>>>(part_t, cg, 32, s->grads + offB[l]);
+        PHIX_LAUNCH_CHECK("reduce_partials");
+        ConvArgs a{};
+        a.B = B; a.H = s->H; a.W = s->W; a.err = s->err;
+        a.x = dz_in; a.wpk = dpk[l]; a.zaux = zprev[l]; a.out = dz_out;
+        conv32_tc<EPI_DGRAD><<<cg, NT, smem_c, st>>>(a);
+        PHIX_LAUNCH_CHECK("conv32_tc<dgrad>");
+        __nv_bfloat16* tmp = dz_in;
+        dz_in = dz_out;
+        dz_out = tmp;
+    }
+    // layer 1 (dz_in now holds dz1)
+    thin_wgrad<<<cg, 320, 0, st>>>(1, nullptr, dz_in, c, B, s->H, s->W, s->P, part_t);
+    PHIX_LAUNCH_CHECK("thin_wgrad(1)");
+    reduce_partials<<<2, 256, 0, st>>>(part_t, cg, 320, t4);
+    PHIX_LAUNCH_CHECK("reduce_partials");
+    PHIX_TRY_CUDA(cudaMemcpyAsync(s->grads + OFF_W1, t4, 288 * 4, cudaMemcpyDeviceToDevice, st));
+    PHIX_TRY_CUDA(cudaMemcpyAsync(s->grads + OFF_B1, t4 + 288, 32 * 4, cudaMemcpyDeviceToDevice, st));
+    // loss
+    std::vector<double> lp(eg);
+    PHIX_TRY_CUDA(cudaMemcpyAsync(lp.data(), s->lpart, sizeof(double) * eg, cudaMemcpyDeviceToHost, st));
+    int herr = 0;
+    PHIX_TRY_CUDA(cudaMemcpyAsync(&herr, s->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PHIX_TRY_CUDA(cudaStreamSynchronize(st));
+    if (herr) { set_error("surrogate: a tensor-core wait timed out"); return PHIX_ERR_CUDA; }
+    double tot = 0.0;
+    for (double v : lp) tot += v;
+    if (loss) *loss = tot / (double)N;
+    return PHIX_OK;
+}
+
+// Adam update of the master parameters with the current gradient vector, then
+// repack the BF16 operands.  `grads` (device, may be null) replaces the
+// internal gradient vector first (data-parallel training passes the averaged
+// gradients here).
+int phix_surrogate_adam(phix_surrogate_t* s, const float* grads, float lr, void* stream) {
+    if (!s) { set_error("adam: NULL"); return PHIX_ERR_ARG; }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (grads) PHIX_TRY_CUDA(cudaMemcpyAsync(s->grads, grads, NPARAM * 4, cudaMemcpyDeviceToDevice, st));
+    s->adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - powf(b1, (float)s->adam_t), c2 = 1.f - powf(b2, (float)s->adam_t);
+    adam_step<<<(NPARAM + 255) / 256, 256, 0, st>>>(s->params, s->grads, s->adam_m, s->adam_v, NPARAM, lr, b1, b2,
+                                                    1e-8f, c1, c2);
+    PHIX_LAUNCH_CHECK("adam_step");
+    return sg_pack(s, st);
+}
+
+// Device pointer of the internal FP32 gradient vector (NPARAM floats).
+float* phix_surrogate_grad_ptr(phix_surrogate_t* s) { return s ? s->grads : nullptr; }
+
+// Compact [H][W] plane <-> 2-D stored FP64 field with ghost g.
+int phix_plane_gather(const double* stored, double* plane, int H, int W, int ghost, void* stream) {
+    if (!stored || !plane || H < 1 || W < 1 || ghost < 0) { set_error("plane_gather: bad argument"); return PHIX_ERR_ARG; }
+    gather_plane<<<dim3((W + 255) / 256, H), 256, 0, (cudaStream_t)stream>>>(stored, plane, H, W, ghost);
+    PHIX_LAUNCH_CHECK("gather_plane");
+    return PHIX_OK;
+}
+int phix_plane_scatter(const double* plane, double* stored, int H, int W, int ghost, void* stream) {
+    if (!stored || !plane || H < 1 || W < 1 || ghost < 0) { set_error("plane_scatter: bad argument"); return PHIX_ERR_ARG; }
+    scatter_plane<<<dim3((W + 255) / 256, H), 256, 0, (cudaStream_t)stream>>>(plane, stored, H, W, ghost);
+    PHIX_LAUNCH_CHECK("scatter_plane");
+    return PHIX_OK;
+}
+
+}  // extern "C"

@@ -63,9 +63,19 @@ def test_golden_cases_vs_reference_gpu(cuda, reference, path):
     assert d <= 1e-12
 
 
+# The reference's CH RK4 step at 1024^2 takes ~53 ms on a B200 (it allocates
+# and zero-fills two host vectors of the full stored size for every composite
+# term evaluation), so the full 20000-step runs take ~20 minutes per config.
+# They run when PHIX_FULL_REFERENCE=1; the default suite runs the full-size
+# grids for fewer steps.
+FULL = os.environ.get("PHIX_FULL_REFERENCE") == "1"
+
+
 @pytest.mark.parametrize("name", ["ac2d", "ch2d"])
 def test_full_size_config_vs_reference_gpu(cuda, reference, name):
     g, phys, prm, scheme, dt, nsteps, fields = getattr(workloads, name)()
+    if not FULL and name == "ch2d":
+        nsteps = 100
     grid = ogrid(g)
     ref = [f.copy() for f in fields]
     ms = reference.advance(ref, phys, prm, scheme, dt, nsteps, grid, use_gpu=True)
@@ -78,6 +88,8 @@ def test_full_size_config_vs_reference_gpu(cuda, reference, name):
 
 def test_full_size_chac3d_vs_reference_gpu(cuda, reference):
     g, phys, prm, scheme, dt, nsteps, fields = workloads.chac3d()
+    if not FULL:
+        nsteps = 4
     grid = ogrid(g)
     ref = [f.copy() for f in fields]
     ms = reference.advance(ref, phys, prm, scheme, dt, nsteps, grid, use_gpu=True)

@@ -1,0 +1,87 @@
+"""Tensor-core surrogate kernels (tcgen05 implicit-GEMM convolutions) against
+the numpy oracle: forward output, all eight gradient tensors, and the exact
+FP64 mean-mass projection.  Tolerances reflect BF16 activations and FP32
+accumulation (the oracle accumulates in FP64)."""
+import numpy as np
+import pytest
+import torch
+
+import phix_b200 as px
+from oracle import surrogate_oracle as so
+
+pytestmark = pytest.mark.gpu
+
+H, W, B = 12, 256, 2
+SHIFT, SCALE, OSCALE = 0.5, 4.0, 0.01
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def setup(seed=0):
+    params = so.init_params(seed)
+    params[6] = params[6] * 10.0  # make the last layer non-trivial for the test
+    params[1] = params[1] + 0.05
+    params[3] = params[3] - 0.02
+    params[5] = params[5] + 0.01
+    params[7] = params[7] + 0.1
+    rng = np.random.default_rng(seed + 1)
+    c = rng.uniform(0.2, 0.8, size=(B, H, W))
+    cn = c + 0.02 * rng.standard_normal((B, H, W))
+    sg = px.Surrogate(H, W, B, SHIFT, SCALE, OSCALE)
+    sg.set_params(px.surrogate_params_to_flat(params))
+    return params, c, cn, sg
+
+
+def test_forward_matches_oracle(cuda):
+    params, c, _, sg = setup()
+    o = torch.empty((B, H, W), dtype=torch.float32, device="cuda")
+    sg.forward(torch.from_numpy(c).cuda(), o)
+    torch.cuda.synchronize()
+    want, _ = so.forward(params, c, SHIFT, SCALE)
+    got = o.cpu().numpy()
+    print("forward rel-L2", rel(got, want))
+    assert rel(got, want) < 1e-2
+    sg.close()
+
+
+def test_gradients_match_oracle(cuda):
+    params, c, cn, sg = setup(3)
+    loss = sg.grad(torch.from_numpy(c).cuda(), torch.from_numpy(cn).cuda())
+    _, g = sg.get_params()
+    o, cache = so.forward(params, c, SHIFT, SCALE)
+    L, do = so.mse_loss_and_grad(o, (cn - c) / OSCALE)
+    want = so.backward(params, cache, do)
+    got = px.surrogate_flat_to_params(g)
+    assert abs(loss - L) <= 2e-2 * L
+    for name, a, b in zip(["W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4"], got, want):
+        r = rel(a.reshape(b.shape), b)
+        print(f"{name}: rel-L2 {r:.3e}")
+        assert r < 5e-2, name
+    sg.close()
+
+
+def test_step_projects_mass_exactly(cuda):
+    params, c, _, sg = setup(5)
+    dc = torch.from_numpy(c).cuda()
+    out = torch.empty_like(dc)
+    sg.step(dc, out)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    for b in range(B):
+        assert abs(got[b].mean() - c[b].mean()) <= 1e-15 * max(1.0, abs(c[b].mean())) * 10
+    want = np.stack([so.step(params, c[b], SHIFT, SCALE, OSCALE) for b in range(B)])
+    assert np.abs(got - want).max() < 1e-2 * OSCALE * 10
+
+
+def test_adam_updates_and_repacks(cuda):
+    params, c, cn, sg = setup(7)
+    dc, dn = torch.from_numpy(c).cuda(), torch.from_numpy(cn).cuda()
+    l0 = sg.grad(dc, dn)
+    for _ in range(20):
+        sg.grad(dc, dn)
+        sg.adam(1e-3)
+    l1 = sg.grad(dc, dn)
+    assert l1 < l0
+    sg.close()
