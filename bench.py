@@ -132,7 +132,7 @@ def bench_ours(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    g, phys, prm, scheme, dt, _, fields = workloads.ch2d()
+    g, phys, prm, scheme, dt, _, fields = workloads.ch2d(n=args.n)
     cells = g.n[0] * g.n[1] * g.n[2]
     prec = px.F64 if args.dtype == "f64" else px.F32
     w = 8 if prec == px.F64 else 4
@@ -182,6 +182,16 @@ def bench_ours(args):
     peak, peak_kind = _peaks()
 
     # e2e through the C ABI with pinned host buffers
+    if args.no_e2e:
+        st.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+                              "ms_per_step": ms_per_step, "roofline_achieved_gbs": achieved, "n": args.n,
+                              "note": "profiling run (--no-e2e)"}), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return None
     h_in = torch.from_numpy(fields[0]).pin_memory()
     h_out = torch.empty_like(h_in).pin_memory()
     for _ in range(2):
@@ -324,6 +334,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="device timing only (profiling runs)")
+    ap.add_argument("--n", type=int, default=1024, help="grid size n x n (the metric is quoted at 1024)")
     ap.add_argument("--cpu-baseline-steps", type=int, default=50)
     ap.add_argument("--ref-sample-steps", type=int, default=2)
     args = ap.parse_args()

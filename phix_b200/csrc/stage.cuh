@@ -206,7 +206,12 @@ __device__ __forceinline__ void box_tile(const StageArgs<T>& A, BoxSmem<T, PHYS,
     const int n0 = A.L.n[0], n1 = A.L.n[1];
     const bool interior = x0 - H >= 0 && x0 + TX + H <= n0 && (DIM < 2 || (y0 - HY >= 0 && y0 + TY + HY <= n1));
 
-    for (int i = threadIdx.x; i < WX * WY; i += NT) {
+    // fixed trip counts: every load of a phase is issued before any is used
+    constexpr int NLOAD = (WX * WY + NT - 1) / NT;
+#pragma unroll
+    for (int it = 0; it < NLOAD; ++it) {
+        const int i = threadIdx.x + it * NT;
+        if (i >= WX * WY) break;
         const int lx = i % WX, ly = i / WX;
         const int px = x0 - H + lx, py = y0 - HY + ly;
 #pragma unroll
@@ -215,7 +220,11 @@ __device__ __forceinline__ void box_tile(const StageArgs<T>& A, BoxSmem<T, PHYS,
     __syncthreads();
 
     if (P::MU) {
-        for (int i = threadIdx.x; i < MX * MY; i += NT) {
+        constexpr int NMU = (MX * MY + NT - 1) / NT;
+#pragma unroll
+        for (int it = 0; it < NMU; ++it) {
+            const int i = threadIdx.x + it * NT;
+            if (i >= MX * MY) break;
             const int lx = i % MX, ly = i / MX;
             const int px = x0 - 1 + lx, py = y0 - (DIM >= 2 ? 1 : 0) + ly;
             int qx = px, qy = py;
@@ -238,7 +247,11 @@ __device__ __forceinline__ void box_tile(const StageArgs<T>& A, BoxSmem<T, PHYS,
         __syncthreads();
     }
 
-    for (int i = threadIdx.x; i < TX * TY; i += NT) {
+    constexpr int NOUT = (TX * TY + NT - 1) / NT;
+#pragma unroll
+    for (int it = 0; it < NOUT; ++it) {
+        const int i = threadIdx.x + it * NT;
+        if (i >= TX * TY) break;
         const int lx = i % TX, ly = i / TX;
         const int px = x0 + lx, py = y0 + ly;
         if (px >= n0 || (DIM >= 2 && py >= n1)) continue;

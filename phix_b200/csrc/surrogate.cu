@@ -41,6 +41,7 @@ constexpr int ROW_B = 4 * CHUNK_B;     // 8320: one staged row, 32 channels
 constexpr int WPK_B = 9 * 2 * 1024;    // packed weights: (tap, k16) blocks of [2][32][8] bf16
 constexpr int DROW_B = 4 * TILE * 16;  // 8192: one un-haloed row (weight-gradient B operand)
 constexpr uint64_t WAIT_NS = 2000000000ull;  // give up on an mbarrier after 2 s
+constexpr int WGRAD_SMEM = 56 * 1024;         // >= 4 * ROW_B + DROW_B + 16; caps residency at 4 CTAs/SM
 
 __device__ __forceinline__ float gelu_f(float x) {
     const float k = 0.7978845608028654f, c = 0.044715f;
@@ -675,6 +676,10 @@ int phix_surrogate_create(phix_surrogate_t** out, int H, int W, int batch_max, d
     auto* s = new (std::nothrow) phix_surrogate();
     if (!s) { set_error("out of host memory"); return PHIX_ERR_ARG; }
     s->H = H; s->W = W; s->bmax = batch_max;
+    {
+        cudaError_t ea = cudaFuncSetAttribute(conv32_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, WGRAD_SMEM);
+        if (ea != cudaSuccess) { delete s; return cuda_status(ea, "cudaFuncSetAttribute(wgrad)"); }
+    }
     s->P.in_shift = in_shift; s->P.in_scale = in_scale; s->P.out_scale = out_scale;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -762,7 +767,9 @@ int phix_surrogate_grad(phix_surrogate_t* s, const double* c, const double* c_ne
     loss_grad<<<eg, 256, 0, st>>>(s->o, c, c_next, s->dO, N, s->P, s->lpart);
     PHIX_LAUNCH_CHECK("loss_grad");
     const int cg = sg_conv_grid(s, B);
-    const size_t smem_c = WPK_B + 3 * ROW_B + 16, smem_w = 4 * ROW_B + DROW_B + 16;
+    // The weight-gradient CTAs hold 128 TMEM columns each; asking for 56 KiB
+    // of shared memory keeps at most 4 of them on an SM (512 columns).
+    const size_t smem_c = WPK_B + 3 * ROW_B + 16, smem_w = WGRAD_SMEM;
     float* part_w = s->partial;                      // cg x 9216
     float* part_t = s->partial + (size_t)cg * 9216;  // cg x 320
     // layer 4
