@@ -13,7 +13,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/phix_b200.h"
+#include "phix_b200.h"
 
 namespace phix {
 
@@ -61,6 +61,21 @@ __device__ __forceinline__ T lap_combine(T tx, T ty, T tz, T i2x, T i2y, T i2z) 
     if (DIM >= 2) v = rfma(ty, i2y, v);
     if (DIM >= 3) v = rfma(tz, i2z, v);
     return v;
+}
+
+// (h, l) += d for a state kept as the unevaluated sum h + l: error-free
+// two-sum of h and d, the error folded into l, then renormalised so that
+// h = fl(h + l).  Used by the FP32 kernels so the state is not rounded to
+// FP32 every step.
+template <typename T>
+__device__ __forceinline__ void twosum_update(T h, T l, T d, T* oh, T* ol) {
+    const T s = radd(h, d);
+    const T bp = rsub(s, h);
+    const T e = radd(rsub(h, rsub(s, bp)), rsub(d, bp));
+    const T l2 = radd(l, e);
+    const T h2 = radd(s, l2);
+    *ol = rsub(l2, rsub(h2, s));
+    *oh = h2;
 }
 
 // Pointwise functors, same operation order as the reference drivers' lambdas.

@@ -19,7 +19,7 @@
 // and mu planes, so every input plane is read once per stage.
 #pragma once
 
-#include "common.cuh"
+#include "phix/detail/common.cuh"
 
 namespace phix {
 
@@ -38,16 +38,66 @@ struct StageArgs {
     const T* k2[2];
     T* out[2];        // k_s, or the new state in the final modes
     T* mu_out;        // MODE_MULTISTEP: the STEADY mu field
+    const T* ulo[2];  // compensated state: low parts of u (null = plain state)
+    T* outlo[2];      // final modes with ulo: low parts of the new state
     T a;              // y = u + a * kin
     T dtf;            // dt/6 (RK4 final) or dt (Euler)
     T i2[3];          // 1/d^2 per axis
     T p[8];           // physics coefficients (make_coeffs in stepper.cu)
 };
 
-template <int PHYS> struct PhysTraits;
-template <> struct PhysTraits<PHIX_PHYS_AC> { static constexpr int NF = 1, H = 1; static constexpr bool MU = false; };
-template <> struct PhysTraits<PHIX_PHYS_CH> { static constexpr int NF = 1, H = 2; static constexpr bool MU = true; };
-template <> struct PhysTraits<PHIX_PHYS_CHAC> { static constexpr int NF = 2, H = 2; static constexpr bool MU = true; };
+// ---------------------------------------------------------------------------
+// Physics policies.  A policy fixes the number of fields NF, the halo H, whether
+// a chemical potential mu (lap(expr, bcs)) is formed on tile+1 (MU), which
+// Laplacians of the stage states the right-hand side needs (LAP_Y0, LAP_Y1),
+// and computes, in the reference's term order,
+//   mu(c, lap c, other field)                          (the inner expression)
+//   rhs(lap mu, y0, lap y0, y1, lap y1) -> k[NF]         (the equation's terms)
+// Built-in policies read their coefficients from StageArgs::p; policies
+// carrying user functors (the C++ DSL) hold them as members.
+// ---------------------------------------------------------------------------
+struct PolAC {  // L*kappa*lap(phi) + L*pw(phi, p - p^3)
+    static constexpr int NF = 1, H = 1;
+    static constexpr bool MU = false, LAP_Y0 = true, LAP_Y1 = false;
+    template <typename T>
+    __device__ __forceinline__ T mu(const StageArgs<T>&, T, T, T) const { return (T)0; }
+    template <typename T>
+    __device__ __forceinline__ void rhs(const StageArgs<T>& A, T, T y0, T lapy0, T, T, T* k) const {
+        k[0] = rfma(A.p[1], f_ac(y0), rfma(A.p[0], lapy0, (T)0));  // rhs = 0; += (L*kappa)*lap; += L*f
+    }
+};
+struct PolCH {  // M*lap(pw(c, f') - kappa*lap(c), bcs)
+    static constexpr int NF = 1, H = 2;
+    static constexpr bool MU = true, LAP_Y0 = false, LAP_Y1 = false;
+    template <typename T>
+    __device__ __forceinline__ T mu(const StageArgs<T>& A, T c, T lapc, T) const {
+        // scratch = 0; scratch += 1*f'(c); scratch += (-kappa)*lap(c)
+        return rfma(A.p[1], lapc, rfma((T)1, f_dw(c, A.p[2], A.p[3], A.p[4]), (T)0));
+    }
+    template <typename T>
+    __device__ __forceinline__ void rhs(const StageArgs<T>& A, T lapmu, T, T, T, T, T* k) const {
+        k[0] = rfma(A.p[0], lapmu, (T)0);  // rhs = 0; rhs += M*lap(mu)
+    }
+};
+struct PolCHAC {  // coupled (c, eta), see PHIX_PHYS_CHAC
+    static constexpr int NF = 2, H = 2;
+    static constexpr bool MU = true, LAP_Y0 = false, LAP_Y1 = true;
+    template <typename T>
+    __device__ __forceinline__ T mu(const StageArgs<T>& A, T c, T lapc, T e) const {
+        return rfma(A.p[1], lapc, rfma((T)1, f_chac_c(c, e, A.p[4]), (T)0));
+    }
+    template <typename T>
+    __device__ __forceinline__ void rhs(const StageArgs<T>& A, T lapmu, T y0, T, T y1, T lapy1, T* k) const {
+        k[0] = rfma(A.p[0], lapmu, (T)0);
+        // rhs = 0; rhs += (-L)*f_eta(eta, c); rhs += (L*kappa_eta)*lap(eta)
+        k[1] = rfma(A.p[2], lapy1, rfma(A.p[3], f_chac_e(y1, y0, A.p[4]), (T)0));
+    }
+};
+
+template <int PHYS> struct PolOf;
+template <> struct PolOf<PHIX_PHYS_AC> { using type = PolAC; };
+template <> struct PolOf<PHIX_PHYS_CH> { using type = PolCH; };
+template <> struct PolOf<PHIX_PHYS_CHAC> { using type = PolCHAC; };
 
 // ---------------------------------------------------------------------------
 // per-cell helpers
@@ -95,61 +145,36 @@ __device__ __forceinline__ int mu_axis(int p, int n, int bc_lo, int bc_hi, doubl
     return MAP_CONST;
 }
 
-// mu = f'(y) - kappa * lap(y) at tile-local point (lx, ly) of y-plane `yc`
-// (with planes `ym`, `yp` below/above in z for 3D).  W = row pitch of the
-// y tile.  Pointwise term first, then the Laplacian, as in the DSL order.
-template <typename T, int PHYS, int DIM, int W>
-__device__ __forceinline__ T compute_mu(const StageArgs<T>& A, const T* yc0, const T* ym0, const T* yp0,
-                                        const T* yc1, int off) {
-    const T c = yc0[off];
-    const T c2 = rmul((T)2, c);
-    T tx = second_diff(yc0[off + 1], c2, yc0[off - 1]);
-    T ty = DIM >= 2 ? second_diff(yc0[off + W], c2, yc0[off - W]) : (T)0;
-    T tz = DIM >= 3 ? second_diff(yp0[off], c2, ym0[off]) : (T)0;
-    T lap = lap_combine<T, DIM>(tx, ty, tz, A.i2[0], A.i2[1], A.i2[2]);
-    T f;
-    if (PHYS == PHIX_PHYS_CH) f = f_dw(c, A.p[2], A.p[3], A.p[4]);
-    else f = f_chac_c(c, yc1[off], A.p[4]);
-    // scratch = 0; scratch += 1*f; scratch += (-kappa)*lap
-    return rfma(A.p[1], lap, rfma((T)1, f, (T)0));
+// Laplacian at offset `off` of a tile plane `c` (pitch W) with z neighbours
+// `m`, `p` (3-D).
+template <typename T, int DIM, int W>
+__device__ __forceinline__ T tile_lap(const StageArgs<T>& A, const T* c, const T* m, const T* p, int off) {
+    const T v2 = rmul((T)2, c[off]);
+    T tx = second_diff(c[off + 1], v2, c[off - 1]);
+    T ty = DIM >= 2 ? second_diff(c[off + W], v2, c[off - W]) : (T)0;
+    T tz = DIM >= 3 ? second_diff(p[off], v2, m[off]) : (T)0;
+    return lap_combine<T, DIM>(tx, ty, tz, A.i2[0], A.i2[1], A.i2[2]);
 }
 
-// Right-hand side of field f at a cell: `m*` are mu planes (CH, CHAC-c) with
-// row pitch MW, `y*` y planes with row pitch W.
-template <typename T, int PHYS, int DIM, int W, int MW>
-__device__ __forceinline__ void compute_rhs(const StageArgs<T>& A, const T* mc, const T* mm, const T* mp, int moff,
-                                            const T* y0c, const T* y0m, const T* y0p, const T* y1c, const T* y1m,
-                                            const T* y1p, int yoff, T* k) {
-    if (PHYS == PHIX_PHYS_AC) {
-        const T p = y0c[yoff];
-        const T p2 = rmul((T)2, p);
-        T tx = second_diff(y0c[yoff + 1], p2, y0c[yoff - 1]);
-        T ty = DIM >= 2 ? second_diff(y0c[yoff + W], p2, y0c[yoff - W]) : (T)0;
-        T tz = DIM >= 3 ? second_diff(y0p[yoff], p2, y0m[yoff]) : (T)0;
-        T lap = lap_combine<T, DIM>(tx, ty, tz, A.i2[0], A.i2[1], A.i2[2]);
-        // rhs = 0; rhs += (L*kappa)*lap; rhs += L*(p - p^3)
-        k[0] = rfma(A.p[1], f_ac(p), rfma(A.p[0], lap, (T)0));
-        return;
-    }
-    {
-        const T m = mc[moff];
-        const T m2 = rmul((T)2, m);
-        T tx = second_diff(mc[moff + 1], m2, mc[moff - 1]);
-        T ty = DIM >= 2 ? second_diff(mc[moff + MW], m2, mc[moff - MW]) : (T)0;
-        T tz = DIM >= 3 ? second_diff(mp[moff], m2, mm[moff]) : (T)0;
-        T lap = lap_combine<T, DIM>(tx, ty, tz, A.i2[0], A.i2[1], A.i2[2]);
-        k[0] = rfma(A.p[0], lap, (T)0);  // rhs = 0; rhs += M*lap(mu)
-    }
-    if (PHYS == PHIX_PHYS_CHAC) {
-        const T e = y1c[yoff];
-        const T e2 = rmul((T)2, e);
-        T tx = second_diff(y1c[yoff + 1], e2, y1c[yoff - 1]);
-        T ty = DIM >= 2 ? second_diff(y1c[yoff + W], e2, y1c[yoff - W]) : (T)0;
-        T tz = DIM >= 3 ? second_diff(y1p[yoff], e2, y1m[yoff]) : (T)0;
-        T lap = lap_combine<T, DIM>(tx, ty, tz, A.i2[0], A.i2[1], A.i2[2]);
-        // rhs = 0; rhs += (-L)*f_eta(eta, c); rhs += (L*kappa_eta)*lap(eta)
-        k[1] = rfma(A.p[2], lap, rfma(A.p[3], f_chac_e(e, y0c[yoff], A.p[4]), (T)0));
-    }
+// mu at tile-local offset `off` of y-plane `yc0` (planes `ym0`, `yp0` below and
+// above in z for 3-D; `yc1` the second field).  W = row pitch of the y tile.
+template <typename T, class Pol, int DIM, int W>
+__device__ __forceinline__ T compute_mu(const StageArgs<T>& A, const Pol& pol, const T* yc0, const T* ym0,
+                                        const T* yp0, const T* yc1, int off) {
+    const T lap = tile_lap<T, DIM, W>(A, yc0, ym0, yp0, off);
+    return pol.mu(A, yc0[off], lap, Pol::NF > 1 ? yc1[off] : (T)0);
+}
+
+// Right-hand side at a cell: `m*` are mu planes (pitch MW), `y*` y planes
+// (pitch W) of fields 0 and 1.
+template <typename T, class Pol, int DIM, int W, int MW>
+__device__ __forceinline__ void compute_rhs(const StageArgs<T>& A, const Pol& pol, const T* mc, const T* mm,
+                                            const T* mp, int moff, const T* y0c, const T* y0m, const T* y0p,
+                                            const T* y1c, const T* y1m, const T* y1p, int yoff, T* k) {
+    const T lapmu = Pol::MU ? tile_lap<T, DIM, MW>(A, mc, mm, mp, moff) : (T)0;
+    const T lapy0 = Pol::LAP_Y0 ? tile_lap<T, DIM, W>(A, y0c, y0m, y0p, yoff) : (T)0;
+    const T lapy1 = Pol::LAP_Y1 ? tile_lap<T, DIM, W>(A, y1c, y1m, y1p, yoff) : (T)0;
+    pol.rhs(A, lapmu, y0c[yoff], lapy0, Pol::NF > 1 ? y1c[yoff] : (T)0, lapy1, k);
 }
 
 // Writes k or the final state for field f at flat index idx.
@@ -158,13 +183,23 @@ __device__ __forceinline__ void emit(const StageArgs<T>& A, int f, int idx, T k)
     if (MODE == MODE_K) {
         A.out[f][idx] = k;
     } else if (MODE == MODE_EULER_FINAL || MODE == MODE_MULTISTEP) {
-        A.out[f][idx] = rfma(A.dtf, k, __ldg(A.u[f] + idx));
+        if (A.ulo[f]) {
+            twosum_update(__ldg(A.u[f] + idx), __ldg(A.ulo[f] + idx), rmul(A.dtf, k), &A.out[f][idx],
+                          &A.outlo[f][idx]);
+        } else {
+            A.out[f][idx] = rfma(A.dtf, k, __ldg(A.u[f] + idx));
+        }
     } else {
         // phi += dt6 * (((k1 + 2 k2) + 2 k3) + k4)
         T s = radd(__ldg(A.k1[f] + idx), rmul((T)2, __ldg(A.k2[f] + idx)));
         s = radd(s, rmul((T)2, __ldg(A.kin[f] + idx)));
         s = radd(s, k);
-        A.out[f][idx] = rfma(A.dtf, s, __ldg(A.u[f] + idx));
+        if (A.ulo[f]) {
+            twosum_update(__ldg(A.u[f] + idx), __ldg(A.ulo[f] + idx), rmul(A.dtf, s), &A.out[f][idx],
+                          &A.outlo[f][idx]);
+        } else {
+            A.out[f][idx] = rfma(A.dtf, s, __ldg(A.u[f] + idx));
+        }
     }
 }
 
@@ -177,16 +212,19 @@ __device__ __forceinline__ void write_ghost(const StageArgs<T>& A, int nf, int p
     double cval;
     int dst = A.L.origin + px + A.L.s[1] * py + A.L.s[2] * pz;
     bool cst = map3<DIM>(A.L, px, py, pz, &src, &cval) == MAP_CONST;
-    for (int f = 0; f < nf; ++f) A.out[f][dst] = cst ? (T)cval : __ldg(A.u[f] + src);
+    for (int f = 0; f < nf; ++f) {
+        A.out[f][dst] = cst ? (T)cval : __ldg(A.u[f] + src);
+        if (A.ulo[f]) A.outlo[f][dst] = cst ? (T)0 : __ldg(A.ulo[f] + src);
+    }
 }
 
 // ---------------------------------------------------------------------------
 // 1-D / 2-D: box tile
 // ---------------------------------------------------------------------------
 // Shared memory of one box tile.
-template <typename T, int PHYS, int DIM, int TX, int TY>
+template <typename T, class Pol, int DIM, int TX, int TY>
 struct BoxSmem {
-    using P = PhysTraits<PHYS>;
+    using P = Pol;
     static constexpr int H = P::H, HY = DIM >= 2 ? P::H : 0;
     static constexpr int WX = TX + 2 * H, WY = TY + 2 * HY;
     static constexpr int MX = TX + 2, MY = TY + (DIM >= 2 ? 2 : 0);
@@ -195,10 +233,11 @@ struct BoxSmem {
 };
 
 // One TX x TY tile whose first physical cell is (x0, y0).
-template <typename T, int PHYS, int DIM, int MODE, int TX, int TY, int NT>
-__device__ __forceinline__ void box_tile(const StageArgs<T>& A, BoxSmem<T, PHYS, DIM, TX, TY>& sm, int x0, int y0) {
-    using P = PhysTraits<PHYS>;
-    using S = BoxSmem<T, PHYS, DIM, TX, TY>;
+template <typename T, class Pol, int DIM, int MODE, int TX, int TY, int NT>
+__device__ __forceinline__ void box_tile(const StageArgs<T>& A, const Pol& pol, BoxSmem<T, Pol, DIM, TX, TY>& sm,
+                                         int x0, int y0) {
+    using P = Pol;
+    using S = BoxSmem<T, Pol, DIM, TX, TY>;
     constexpr int NF = P::NF, H = S::H, HY = S::HY, WX = S::WX, WY = S::WY, MX = S::MX, MY = S::MY;
     T(&ys)[NF][WY * WX] = sm.ys;
     T* ms = sm.ms;
@@ -240,7 +279,7 @@ __device__ __forceinline__ void box_tile(const StageArgs<T>& A, BoxSmem<T, PHYS,
                 v = (T)cval;
             } else {
                 const int off = (qx - x0 + H) + (qy - y0 + HY) * WX;
-                v = compute_mu<T, PHYS, DIM, WX>(A, ys[0], nullptr, nullptr, ys[NF - 1], off);
+                v = compute_mu<T, Pol, DIM, WX>(A, pol, ys[0], nullptr, nullptr, ys[NF - 1], off);
             }
             ms[i] = v;
         }
@@ -258,8 +297,8 @@ __device__ __forceinline__ void box_tile(const StageArgs<T>& A, BoxSmem<T, PHYS,
         const int yoff = (lx + H) + (ly + HY) * WX;
         const int moff = (lx + 1) + (ly + (DIM >= 2 ? 1 : 0)) * MX;
         T k[2];
-        compute_rhs<T, PHYS, DIM, WX, MX>(A, ms, nullptr, nullptr, moff, ys[0], nullptr, nullptr, ys[NF - 1],
-                                          nullptr, nullptr, yoff, k);
+        compute_rhs<T, Pol, DIM, WX, MX>(A, pol, ms, nullptr, nullptr, moff, ys[0], nullptr, nullptr, ys[NF - 1],
+                                         nullptr, nullptr, yoff, k);
         const int idx = A.L.origin + px + A.L.s[1] * py;
 #pragma unroll
         for (int f = 0; f < NF; ++f) emit<T, MODE>(A, f, idx, k[f]);
@@ -305,10 +344,10 @@ __device__ __forceinline__ void box_tile(const StageArgs<T>& A, BoxSmem<T, PHYS,
 }
 
 // Single field: one CTA per tile.
-template <typename T, int PHYS, int DIM, int MODE, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) stage_box(const StageArgs<T> A) {
-    __shared__ BoxSmem<T, PHYS, DIM, TX, TY> sm;
-    box_tile<T, PHYS, DIM, MODE, TX, TY, NT>(A, sm, blockIdx.x * TX, blockIdx.y * TY);
+template <typename T, class Pol, int DIM, int MODE, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) stage_box(const StageArgs<T> A, const Pol pol) {
+    __shared__ BoxSmem<T, Pol, DIM, TX, TY> sm;
+    box_tile<T, Pol, DIM, MODE, TX, TY, NT>(A, pol, sm, blockIdx.x * TX, blockIdx.y * TY);
 }
 
 // Many independent fields in one persistent launch: CTA b walks the tile list
@@ -318,13 +357,14 @@ struct BatchTile {
     int inst, x0, y0, pad;
 };
 
-template <typename T, int PHYS, int MODE, int TX, int TY, int NT>
+template <typename T, class Pol, int MODE, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT) stage_box_batched(const StageArgs<T>* __restrict__ args,
-                                                        const BatchTile* __restrict__ tiles, int ntiles) {
-    __shared__ BoxSmem<T, PHYS, 2, TX, TY> sm;
+                                                        const BatchTile* __restrict__ tiles, int ntiles,
+                                                        const Pol pol) {
+    __shared__ BoxSmem<T, Pol, 2, TX, TY> sm;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const BatchTile bt = tiles[t];
-        box_tile<T, PHYS, 2, MODE, TX, TY, NT>(args[bt.inst], sm, bt.x0, bt.y0);
+        box_tile<T, Pol, 2, MODE, TX, TY, NT>(args[bt.inst], pol, sm, bt.x0, bt.y0);
         __syncthreads();  // shared memory is reused by the next tile
     }
 }
@@ -332,23 +372,23 @@ __global__ void __launch_bounds__(NT) stage_box_batched(const StageArgs<T>* __re
 // ---------------------------------------------------------------------------
 // 3-D: in-plane tile marching along z
 // ---------------------------------------------------------------------------
-template <typename T, int PHYS, int TX, int TY>
+template <typename T, class Pol, int TX, int TY>
 struct March3D {
-    static constexpr int NF = PhysTraits<PHYS>::NF, H = PhysTraits<PHYS>::H;
+    static constexpr int NF = Pol::NF, H = Pol::H;
     static constexpr int WX = TX + 2 * H, WY = TY + 2 * H, WP = WX * WY;  // y plane
     static constexpr int MX = TX + 2, MY = TY + 2, MP = MX * MY;         // mu plane
     static constexpr int NYR = 5, NMR = 4;                               // ring depths
     static constexpr size_t smem_bytes() {
-        return sizeof(T) * ((size_t)NF * NYR * WP + (PhysTraits<PHYS>::MU ? (size_t)NMR * MP : 0));
+        return sizeof(T) * ((size_t)NF * NYR * WP + (Pol::MU ? (size_t)NMR * MP : 0));
     }
 };
 
-template <typename T, int PHYS, int MODE, int TX, int TY, int RZ, int NT>
-__global__ void __launch_bounds__(NT) stage_march3d(const StageArgs<T> A) {
-    using G = March3D<T, PHYS, TX, TY>;
+template <typename T, class Pol, int MODE, int TX, int TY, int RZ, int NT>
+__global__ void __launch_bounds__(NT) stage_march3d(const StageArgs<T> A, const Pol pol) {
+    using G = March3D<T, Pol, TX, TY>;
     constexpr int NF = G::NF, H = G::H, WX = G::WX, WP = G::WP, MX = G::MX, MP = G::MP;
     constexpr int NYR = G::NYR, NMR = G::NMR;
-    constexpr bool MU = PhysTraits<PHYS>::MU;
+    constexpr bool MU = Pol::MU;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* ysb = reinterpret_cast<T*>(smem_raw);   // [NF][NYR][WP]
     T* msb = ysb + (size_t)NF * NYR * WP;      // [NMR][MP]
@@ -391,7 +431,7 @@ __global__ void __launch_bounds__(NT) stage_march3d(const StageArgs<T> A) {
                 v = (T)cval;
             } else {
                 const int off = (qx - x0 + H) + (qy - y0 + H) * WX;
-                v = compute_mu<T, PHYS, 3, WX>(A, yslot(0, qz), yslot(0, qz - 1), yslot(0, qz + 1),
+                v = compute_mu<T, Pol, 3, WX>(A, pol, yslot(0, qz), yslot(0, qz - 1), yslot(0, qz + 1),
                                                yslot(NF - 1, qz), off);
             }
             dst[i] = v;
@@ -426,7 +466,7 @@ __global__ void __launch_bounds__(NT) stage_march3d(const StageArgs<T> A) {
             const int yoff = (lx + H) + (ly + H) * WX;
             const int moff = (lx + 1) + (ly + 1) * MX;
             T k[2];
-            compute_rhs<T, PHYS, 3, WX, MX>(A, mslot(z), mslot(z - 1), mslot(z + 1), moff, y0c, y0m, y0p, y1c,
+            compute_rhs<T, Pol, 3, WX, MX>(A, pol, mslot(z), mslot(z - 1), mslot(z + 1), moff, y0c, y0m, y0p, y1c,
                                             y1m, y1p, yoff, k);
             const int idx = A.L.origin + px + A.L.s[1] * py + A.L.s[2] * z;
 #pragma unroll

@@ -117,6 +117,9 @@ class Oracle:
             getattr(L, "or_advance" + sfx).argtypes = [PP, C.c_int, C.POINTER(C.c_double), C.c_int,
                                                        C.c_double, C.c_int, g]
             getattr(L, "or_advance" + sfx).restype = C.c_int
+            getattr(L, "or_advance_comp" + sfx).argtypes = [PP, PP, C.c_int, C.POINTER(C.c_double), C.c_int,
+                                                            C.c_double, C.c_int, g]
+            getattr(L, "or_advance_comp" + sfx).restype = C.c_int
             getattr(L, "or_advance_ch_multistep" + sfx).argtypes = [P, P, C.POINTER(C.c_double), C.c_double,
                                                                     C.c_int, g]
             getattr(L, "or_axpy" + sfx).argtypes = [P, P, C.c_double, C.c_long, C.c_int]
@@ -179,6 +182,16 @@ class Oracle:
         rc = getattr(self.lib, "or_advance" + s)(self._pp(fields, ct), phys, p, scheme, dt, nsteps, C.byref(gt))
         if rc != 0:
             raise RuntimeError(f"or_advance failed: {rc}")
+
+    def advance_comp(self, hi, lo, phys, prm, scheme, dt, nsteps, grid: Grid, fma_mode=None):
+        """Compensated (hi + lo) state, the FP32 kernels' scheme."""
+        s, ct = self._sfx(hi[0])
+        gt = grid.ctype(fma_mode)
+        p = (C.c_double * 8)(*(list(prm) + [0.0] * (8 - len(prm))))
+        rc = getattr(self.lib, "or_advance_comp" + s)(self._pp(hi, ct), self._pp(lo, ct), phys, p, scheme, dt,
+                                                      nsteps, C.byref(gt))
+        if rc != 0:
+            raise RuntimeError(f"or_advance_comp failed: {rc}")
 
     def advance_ch_multistep(self, c, mu, prm, dt, nsteps, grid: Grid, fma_mode=None):
         s, ct = self._sfx(c)

@@ -311,6 +311,75 @@ int FN(or_advance)(REAL** u, int phys, const double* prm, int scheme,
 }
 
 /* ---------------------------------------------------------------------------
+ * Compensated state (the FP32 kernels' scheme): the state is the unevaluated
+ * sum hi + lo of two REALs.  Stage states and right-hand sides use hi only,
+ * exactly as or_advance does; the final update adds delta = dt*k (Euler) or
+ * dt/6*(k1+2k2+2k3+k4) (RK4) to (hi, lo) with an error-free two-sum and a
+ * renormalisation, so the state itself is not rounded to REAL each step.
+ * BCs refresh the ghosts of hi at the start of each step; lo never enters a
+ * stencil, so its ghosts are left as they are.
+ * ------------------------------------------------------------------------- */
+static inline void FN(twosum_update)(REAL* h, REAL* l, REAL d) {
+    volatile REAL s = *h + d;
+    volatile REAL bp = s - *h;
+    volatile REAL e = (*h - (s - bp)) + (d - bp);
+    volatile REAL l2 = *l + e;
+    volatile REAL h2 = s + l2;
+    *l = l2 - (h2 - s);
+    *h = h2;
+}
+
+int FN(or_advance_comp)(REAL** hi, REAL** lo, int phys, const double* prm, int scheme, double dt, int nsteps,
+                        const or_grid_t* g) {
+    long S = FN(stored)(g);
+    int nf = FN(nfields)(phys), mode = g->fma_mode;
+    REAL* buf = (REAL*)calloc((size_t)S * (2 + 5 * nf), sizeof(REAL));
+    if (!buf) return -1;
+    REAL* scratch = buf;
+    REAL *k1[2], *k2[2], *k3[2], *k4[2], *tmp[2];
+    for (int f = 0; f < nf; ++f) {
+        k1[f] = buf + S * (1 + 5 * f + 0);
+        k2[f] = buf + S * (1 + 5 * f + 1);
+        k3[f] = buf + S * (1 + 5 * f + 2);
+        k4[f] = buf + S * (1 + 5 * f + 3);
+        tmp[f] = buf + S * (1 + 5 * f + 4);
+    }
+    REAL dtr = (REAL)dt;
+    REAL dt2 = (REAL)(dt * 0.5), dt6 = (REAL)(dt / 6.0);
+    for (int s = 0; s < nsteps; ++s) {
+        for (int f = 0; f < nf; ++f) FN(or_bc_apply)(hi[f], g);
+        FN(or_rhs)(k1, hi, phys, prm, g, scratch);
+        if (scheme == OR_EULER) {
+            for (int f = 0; f < nf; ++f)
+                for (long i = 0; i < S; ++i) {
+                    volatile REAL d = dtr * k1[f][i];
+                    FN(twosum_update)(&hi[f][i], &lo[f][i], d);
+                }
+            continue;
+        }
+        REAL** ks[3] = {k1, k2, k3};
+        REAL** kn[3] = {k2, k3, k4};
+        REAL as[3] = {dt2, dt2, dtr};
+        for (int st = 0; st < 3; ++st) {
+            for (int f = 0; f < nf; ++f) {
+                for (long i = 0; i < S; ++i) tmp[f][i] = FN(madd)(mode, as[st], ks[st][f][i], hi[f][i]);
+                FN(or_bc_apply)(tmp[f], g);
+            }
+            FN(or_rhs)(kn[st], tmp, phys, prm, g, scratch);
+        }
+        for (int f = 0; f < nf; ++f)
+            for (long i = 0; i < S; ++i) {
+                REAL a = (k1[f][i] + (REAL)2 * k2[f][i]) + (REAL)2 * k3[f][i];
+                a = a + k4[f][i];
+                volatile REAL d = dt6 * a;
+                FN(twosum_update)(&hi[f][i], &lo[f][i], d);
+            }
+    }
+    free(buf);
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------
  * Multi-step Euler (Solver.cu:317-340) for the shipped Cahn-Hilliard app
  * (Cahn-Hillard_double-well.cu:84-106):
  *   step 1 (STEADY)   : BCs on c, mu = pw(c, f') - kappa*lap(c)

@@ -306,17 +306,32 @@ class Batch:
         except Exception:
             pass
 
+    def _check_field(self, inst: int, field):
+        if not 0 <= inst < self.n:
+            raise IndexError(f"batch instance {inst} out of range [0, {self.n})")
+        want = int(np.prod(stored_shape(self.grids[inst])))
+        if isinstance(field, np.ndarray):
+            ok = field.dtype == np.float64 and field.flags["C_CONTIGUOUS"]
+        else:
+            import torch
+            ok = field.dtype == torch.float64 and field.is_contiguous()
+        if not ok:
+            raise ValueError("batch field must be a contiguous float64 array")
+        n = field.size if isinstance(field, np.ndarray) else field.numel()
+        if n != want:
+            raise ValueError(f"batch instance {inst}: field has {n} values, its stored grid has {want}")
+
     def load(self, inst: int, field, stream=None):
         """field: FP64 stored array; numpy (host) or CUDA tensor (device)."""
+        self._check_field(inst, field)
         if isinstance(field, np.ndarray):
-            assert field.dtype == np.float64 and field.flags["C_CONTIGUOUS"]
             check(lib().phix_batch_load(self.h, inst, C.c_void_p(field.ctypes.data), 1, _stream(stream)))
         else:
             check(lib().phix_batch_load(self.h, inst, _dev(field), 0, _stream(stream)))
 
     def store(self, inst: int, field, stream=None):
+        self._check_field(inst, field)
         if isinstance(field, np.ndarray):
-            assert field.dtype == np.float64 and field.flags["C_CONTIGUOUS"]
             check(lib().phix_batch_store(self.h, inst, C.c_void_p(field.ctypes.data), 1, _stream(stream)))
         else:
             check(lib().phix_batch_store(self.h, inst, _dev(field), 0, _stream(stream)))

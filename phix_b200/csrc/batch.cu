@@ -14,8 +14,8 @@
 #include <new>
 #include <vector>
 
-#include "common.cuh"
-#include "stage.cuh"
+#include "phix/detail/common.cuh"
+#include "phix/detail/stage.cuh"
 #include "stepper.h"
 
 namespace phix {
@@ -31,13 +31,14 @@ constexpr int kNumTileCfgs = sizeof(kTileCfgs) / sizeof(kTileCfgs[0]);
 template <typename T, int PHYS, int MODE, int TX, int TY, int NT>
 int launch_batched_cfg(const StageArgs<T>* args, const BatchTile* tiles, int ntiles, int ctas_per_sm, int nsm,
                        cudaStream_t s) {
-    auto kern = stage_box_batched<T, PHYS, MODE, TX, TY, NT>;
+    using Pol = typename PolOf<PHYS>::type;
+    auto kern = stage_box_batched<T, Pol, MODE, TX, TY, NT>;
     int occ = 0;
     PHIX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, 0));
     int per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, std::max(occ, 1)) : std::max(occ, 1);
     int grid = std::min(ntiles, nsm * per_sm);
     if (grid < 1) grid = 1;
-    kern<<<grid, NT, 0, s>>>(args, tiles, ntiles);
+    kern<<<grid, NT, 0, s>>>(args, tiles, ntiles, Pol{});
     PHIX_LAUNCH_CHECK("stage_box_batched");
     return PHIX_OK;
 }
@@ -131,6 +132,7 @@ struct phix_batch {
     std::vector<double> prm;          // ninst x 8
     void* pool = nullptr;             // all buffers
     std::vector<void*> st[2], kb[3];  // per instance (field 0 only: batch supports 1-field physics)
+    std::vector<void*> lo[2];         // FP32: low parts of the compensated state
     int cur = 0;
     int cfg = 0, ctas_per_sm = 0, nsm = 148;
     // device-side argument tables: [stage kind][parity] -> ninst StageArgs
@@ -240,6 +242,10 @@ int build_args(phix_batch* b) {
                     A.out[0] = (T*)b->st[1 - par][i];
                     A.dtf = (T)b->dt;
                 }
+                if (kind >= 3 && b->lo[0][i]) {
+                    A.ulo[0] = (const T*)b->lo[par][i];
+                    A.outlo[0] = (T*)b->lo[1 - par][i];
+                }
             }
     if (!b->args_dev) {
         b->args_bytes = sizeof(StageArgs<T>) * n;
@@ -330,8 +336,10 @@ int phix_batch_create(phix_batch_t** out, int phys, int scheme, int precision, i
         if (!rc && grids[i].dim != 2) { set_error("batch: instance %d is not 2-D", i); rc = PHIX_ERR_UNSUPPORTED; }
         if (rc) { delete b; return rc; }
     }
-    // pool: per instance 2 states + 3 k (RK4), each padded to 256 bytes
-    const int nbuf = scheme == PHIX_RK4 ? 5 : 2;
+    // pool: per instance 2 states (+ 2 low parts in FP32) + 3 k (RK4), each
+    // padded to 256 bytes
+    const int nlo = precision == PHIX_F32 ? 2 : 0;
+    const int nbuf = (scheme == PHIX_RK4 ? 5 : 2) + nlo;
     size_t total = 0;
     std::vector<size_t> off(ninst);
     for (int i = 0; i < ninst; ++i) {
@@ -342,6 +350,7 @@ int phix_batch_create(phix_batch_t** out, int phys, int scheme, int precision, i
     if (e != cudaSuccess) { delete b; return cuda_status(e, "cudaMalloc(batch pool)"); }
     cudaMemset(b->pool, 0, total);
     for (int k = 0; k < 2; ++k) b->st[k].resize(ninst);
+    for (int k = 0; k < 2; ++k) b->lo[k].resize(ninst, nullptr);
     for (int k = 0; k < 3; ++k) b->kb[k].resize(ninst, nullptr);
     for (int i = 0; i < ninst; ++i) {
         const size_t sz = (b->stored[i] * b->esz + 255) / 256 * 256;
@@ -350,6 +359,11 @@ int phix_batch_create(phix_batch_t** out, int phys, int scheme, int precision, i
         b->st[1][i] = base + sz;
         if (scheme == PHIX_RK4)
             for (int k = 0; k < 3; ++k) b->kb[k][i] = base + (2 + k) * sz;
+        if (nlo) {
+            char* lb = base + (nbuf - 2) * sz;
+            b->lo[0][i] = lb;
+            b->lo[1][i] = lb + sz;
+        }
     }
     int dev = 0;
     cudaGetDevice(&dev);
@@ -396,12 +410,16 @@ int phix_batch_load(phix_batch_t* b, int inst, const double* field, int from_hos
             PHIX_TRY_CUDA(cudaMemcpyAsync(dst, field, S * 8, from_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
         } else {
             if (from_host) {
-                std::vector<float> tmp(S);
-                for (size_t q = 0; q < S; ++q) tmp[q] = (float)field[q];
-                PHIX_TRY_CUDA(cudaMemcpyAsync(dst, tmp.data(), S * 4, cudaMemcpyHostToDevice, s));
+                std::vector<float> th(S), tl(S);
+                for (size_t q = 0; q < S; ++q) {
+                    th[q] = (float)field[q];
+                    tl[q] = (float)(field[q] - (double)th[q]);
+                }
+                PHIX_TRY_CUDA(cudaMemcpyAsync(dst, th.data(), S * 4, cudaMemcpyHostToDevice, s));
+                PHIX_TRY_CUDA(cudaMemcpyAsync(b->lo[k][inst], tl.data(), S * 4, cudaMemcpyHostToDevice, s));
                 PHIX_TRY_CUDA(cudaStreamSynchronize(s));
             } else {
-                int rc = convert_f64_to_f32((float*)dst, field, S, s);
+                int rc = convert_f64_split((float*)dst, (float*)b->lo[k][inst], field, S, s);
                 if (rc) return rc;
             }
         }
@@ -419,14 +437,16 @@ int phix_batch_store(phix_batch_t* b, int inst, double* field, int to_host, void
         if (to_host) PHIX_TRY_CUDA(cudaStreamSynchronize(s));
         return PHIX_OK;
     }
+    const void* lsrc = b->lo[b->cur][inst];
     if (to_host) {
-        std::vector<float> tmp(S);
-        PHIX_TRY_CUDA(cudaMemcpyAsync(tmp.data(), src, S * 4, cudaMemcpyDeviceToHost, s));
+        std::vector<float> th(S), tl(S);
+        PHIX_TRY_CUDA(cudaMemcpyAsync(th.data(), src, S * 4, cudaMemcpyDeviceToHost, s));
+        PHIX_TRY_CUDA(cudaMemcpyAsync(tl.data(), lsrc, S * 4, cudaMemcpyDeviceToHost, s));
         PHIX_TRY_CUDA(cudaStreamSynchronize(s));
-        for (size_t q = 0; q < S; ++q) field[q] = (double)tmp[q];
+        for (size_t q = 0; q < S; ++q) field[q] = (double)th[q] + (double)tl[q];
         return PHIX_OK;
     }
-    return convert_f32_to_f64(field, (const float*)src, S, s);
+    return convert_pair_to_f64(field, (const float*)src, (const float*)lsrc, S, s);
 }
 
 int phix_batch_set_tiles(phix_batch_t* b, int tile_cfg, int ctas_per_sm) {
@@ -473,15 +493,18 @@ int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms) {
     if (!b || trial_steps < 1) { set_error("batch_autotune: bad argument"); return PHIX_ERR_ARG; }
     // The state evolves during trials; save and restore it so tuning is invisible.
     const int cur0 = b->cur;
+    const int parts = b->lo[0][0] ? 2 : 1;
     size_t bytes = 0;
-    for (int i = 0; i < b->ninst; ++i) bytes += b->stored[i] * b->esz;
+    for (int i = 0; i < b->ninst; ++i) bytes += parts * b->stored[i] * b->esz;
     void* save = nullptr;
     PHIX_TRY_CUDA(cudaMalloc(&save, bytes));
     size_t o = 0;
-    for (int i = 0; i < b->ninst; ++i) {
-        PHIX_TRY_CUDA(cudaMemcpy((char*)save + o, b->st[cur0][i], b->stored[i] * b->esz, cudaMemcpyDeviceToDevice));
-        o += b->stored[i] * b->esz;
-    }
+    for (int i = 0; i < b->ninst; ++i)
+        for (int q = 0; q < parts; ++q) {
+            const void* src = q ? b->lo[cur0][i] : b->st[cur0][i];
+            PHIX_TRY_CUDA(cudaMemcpy((char*)save + o, src, b->stored[i] * b->esz, cudaMemcpyDeviceToDevice));
+            o += b->stored[i] * b->esz;
+        }
     const int old_graph = b->graph_steps;
     b->graph_steps = 0;
     cudaEvent_t e0, e1;
@@ -509,10 +532,12 @@ int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms) {
     // restore the state into the buffer that was current
     b->cur = cur0;
     o = 0;
-    for (int i = 0; i < b->ninst; ++i) {
-        cudaMemcpy(b->st[cur0][i], (char*)save + o, b->stored[i] * b->esz, cudaMemcpyDeviceToDevice);
-        o += b->stored[i] * b->esz;
-    }
+    for (int i = 0; i < b->ninst; ++i)
+        for (int q = 0; q < parts; ++q) {
+            void* dst = q ? b->lo[cur0][i] : b->st[cur0][i];
+            cudaMemcpy(dst, (char*)save + o, b->stored[i] * b->esz, cudaMemcpyDeviceToDevice);
+            o += b->stored[i] * b->esz;
+        }
     cudaFree(save);
     b->graph_steps = old_graph;
     if (rc) return rc;

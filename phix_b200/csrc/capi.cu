@@ -4,7 +4,7 @@
 #include <cstdarg>
 #include <cstdio>
 
-#include "common.cuh"
+#include "phix/detail/common.cuh"
 
 namespace phix {
 

@@ -3,7 +3,7 @@
 #include <cstdint>
 #include <cstring>
 
-#include "common.cuh"
+#include "phix/detail/common.cuh"
 #include "stepper.h"
 
 namespace phix {
@@ -39,6 +39,23 @@ __global__ void __launch_bounds__(256) f32_to_f64(double* __restrict__ dst, cons
     if (i < n) dst[i] = (double)src[i];
 }
 
+// hi[i] = (float)x[i], lo[i] = (float)(x[i] - hi[i]): x split into an
+// unevaluated float pair (the compensated FP32 state).
+__global__ void __launch_bounds__(256) f64_split_f32(float* __restrict__ hi, float* __restrict__ lo,
+                                                     const double* __restrict__ x, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double v = x[i];
+        const float h = (float)v;
+        hi[i] = h;
+        lo[i] = (float)(v - (double)h);
+    }
+}
+__global__ void __launch_bounds__(256) f32_pair_to_f64(double* __restrict__ x, const float* __restrict__ hi,
+                                                       const float* __restrict__ lo, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        x[i] = (double)hi[i] + (double)lo[i];
+}
+
 static int aligned16(const void* a, const void* b) {
     return ((uintptr_t)a % 16 == 0) && ((uintptr_t)b % 16 == 0);
 }
@@ -61,6 +78,18 @@ int convert_f32_to_f64(double* dst, const float* src, size_t n, cudaStream_t s) 
     return PHIX_OK;
 }
 
+int convert_f64_split(float* hi, float* lo, const double* src, size_t n, cudaStream_t s) {
+    f64_split_f32<<<conv_grid(n), 256, 0, s>>>(hi, lo, src, n);
+    PHIX_LAUNCH_CHECK("f64_split_f32");
+    return PHIX_OK;
+}
+
+int convert_pair_to_f64(double* dst, const float* hi, const float* lo, size_t n, cudaStream_t s) {
+    f32_pair_to_f64<<<conv_grid(n), 256, 0, s>>>(dst, hi, lo, n);
+    PHIX_LAUNCH_CHECK("f32_pair_to_f64");
+    return PHIX_OK;
+}
+
 int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s) {
     const size_t S = stepper_stored(h);
     for (int f = 0; f < stepper_nf(h); ++f) {
@@ -74,6 +103,9 @@ int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s
             if (stepper_prec(h) == PHIX_F64) {
                 if (dst == (const void*)fields[f]) continue;
                 PHIX_TRY_CUDA(cudaMemcpyAsync(dst, fields[f], S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            } else if (stepper_lo_buf(h, b, f)) {
+                f64_split_f32<<<conv_grid(S), 256, 0, s>>>((float*)dst, (float*)stepper_lo_buf(h, b, f), fields[f], S);
+                PHIX_LAUNCH_CHECK("f64_split_f32");
             } else {
                 f64_to_f32<<<conv_grid(S), 256, 0, s>>>((float*)dst, fields[f], S, aligned16(dst, fields[f]));
                 PHIX_LAUNCH_CHECK("f64_to_f32");
@@ -93,8 +125,15 @@ int stepper_copy_out(phix_stepper* h, double* const* fields, cudaStream_t s) {
             if (src == (const void*)fields[f]) continue;
             PHIX_TRY_CUDA(cudaMemcpyAsync(fields[f], src, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
         } else {
-            f32_to_f64<<<conv_grid(S), 256, 0, s>>>(fields[f], (const float*)src, S, aligned16(src, fields[f]));
-            PHIX_LAUNCH_CHECK("f32_to_f64");
+            const bool multi_mu = stepper_scheme(h) == PHIX_MULTISTEP && f == 1;
+            const void* lo = multi_mu ? nullptr : stepper_lo_buf(h, stepper_cur(h), f);
+            if (lo) {
+                f32_pair_to_f64<<<conv_grid(S), 256, 0, s>>>(fields[f], (const float*)src, (const float*)lo, S);
+                PHIX_LAUNCH_CHECK("f32_pair_to_f64");
+            } else {
+                f32_to_f64<<<conv_grid(S), 256, 0, s>>>(fields[f], (const float*)src, S, aligned16(src, fields[f]));
+                PHIX_LAUNCH_CHECK("f32_to_f64");
+            }
         }
     }
     return PHIX_OK;
@@ -106,8 +145,15 @@ int stepper_diag(phix_stepper* h, double* out) {
     double* part = stepper_partials(h, np);
     if (!part) { set_error("diagnostics: cudaMalloc failed"); return PHIX_ERR_CUDA; }
     if (stepper_prec(h) == PHIX_F32) {
-        const float* f[2] = {(const float*)stepper_state(h, 0), nf > 1 ? (const float*)stepper_state(h, 1) : nullptr};
-        return reduce_mass_energy<float>(f, nf, stepper_phys(h), stepper_prm(h), stepper_grid(h), part, np, out, 0);
+        // FP64 value of the compensated state (hi + lo) in the staging buffer
+        double* stage = stepper_staging(h);
+        if (!stage) { set_error("diagnostics: cudaMalloc(staging) failed"); return PHIX_ERR_CUDA; }
+        const size_t S = stepper_stored(h);
+        double* outs[2] = {stage, stage + S};
+        int rc = stepper_copy_out(h, outs, 0);
+        if (rc) return rc;
+        const double* f[2] = {stage, nf > 1 ? stage + S : nullptr};
+        return reduce_mass_energy<double>(f, nf, stepper_phys(h), stepper_prm(h), stepper_grid(h), part, np, out, 0);
     }
     const double* f[2] = {(const double*)stepper_state(h, 0), nf > 1 ? (const double*)stepper_state(h, 1) : nullptr};
     return reduce_mass_energy<double>(f, nf, stepper_phys(h), stepper_prm(h), stepper_grid(h), part, np, out, 0);

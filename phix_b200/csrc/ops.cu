@@ -3,7 +3,7 @@
 // axpy.  Each replaces one of the reference's per-term kernels with the same
 // arithmetic (rounding pinned as in stage.cuh) on a 2-D/3-D launch grid
 // instead of the reference's 1-D grid with div/mod index recovery.
-#include "common.cuh"
+#include "phix/detail/common.cuh"
 #include "stepper.h"
 
 namespace phix {

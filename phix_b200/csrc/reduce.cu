@@ -12,7 +12,7 @@
 // given grid.  Non-finite cells are counted, not trapped.
 #include <cmath>
 
-#include "common.cuh"
+#include "phix/detail/common.cuh"
 #include "stepper.h"
 
 namespace phix {

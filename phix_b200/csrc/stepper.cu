@@ -14,8 +14,8 @@
 #include <new>
 #include <vector>
 
-#include "common.cuh"
-#include "stage.cuh"
+#include "phix/detail/common.cuh"
+#include "phix/detail/stage.cuh"
 #include "stepper.h"
 
 namespace phix {
@@ -31,12 +31,13 @@ constexpr int M3_TX = 32, M3_TY = 8, M3_RZ = 16, M3_NT = 256;
 
 template <typename T, int PHYS, int DIM, int MODE>
 int launch_box(const StageArgs<T>& A, cudaStream_t s) {
+    using Pol = typename PolOf<PHYS>::type;
     if (DIM == 1) {
         dim3 grid((A.L.n[0] + LIN_TX - 1) / LIN_TX, 1, 1);
-        stage_box<T, PHYS, 1, MODE, LIN_TX, 1, LIN_NT><<<grid, LIN_NT, 0, s>>>(A);
+        stage_box<T, Pol, 1, MODE, LIN_TX, 1, LIN_NT><<<grid, LIN_NT, 0, s>>>(A, Pol{});
     } else {
         dim3 grid((A.L.n[0] + BOX_TX - 1) / BOX_TX, (A.L.n[1] + BOX_TY - 1) / BOX_TY, 1);
-        stage_box<T, PHYS, 2, MODE, BOX_TX, BOX_TY, BOX_NT><<<grid, BOX_NT, 0, s>>>(A);
+        stage_box<T, Pol, 2, MODE, BOX_TX, BOX_TY, BOX_NT><<<grid, BOX_NT, 0, s>>>(A, Pol{});
     }
     PHIX_LAUNCH_CHECK("stage_box");
     return PHIX_OK;
@@ -46,8 +47,9 @@ int launch_box(const StageArgs<T>& A, cudaStream_t s) {
 // creation (never inside a stream capture).
 template <typename T, int PHYS, int MODE>
 int prepare_march() {
-    using G = March3D<T, PHYS, M3_TX, M3_TY>;
-    auto kern = stage_march3d<T, PHYS, MODE, M3_TX, M3_TY, M3_RZ, M3_NT>;
+    using Pol = typename PolOf<PHYS>::type;
+    using G = March3D<T, Pol, M3_TX, M3_TY>;
+    auto kern = stage_march3d<T, Pol, MODE, M3_TX, M3_TY, M3_RZ, M3_NT>;
     PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
     return PHIX_OK;
 }
@@ -71,11 +73,12 @@ int prepare_t(int phys) {
 
 template <typename T, int PHYS, int MODE>
 int launch_march(const StageArgs<T>& A, cudaStream_t s) {
-    using G = March3D<T, PHYS, M3_TX, M3_TY>;
-    auto kern = stage_march3d<T, PHYS, MODE, M3_TX, M3_TY, M3_RZ, M3_NT>;
+    using Pol = typename PolOf<PHYS>::type;
+    using G = March3D<T, Pol, M3_TX, M3_TY>;
+    auto kern = stage_march3d<T, Pol, MODE, M3_TX, M3_TY, M3_RZ, M3_NT>;
     const size_t smem = G::smem_bytes();
     dim3 grid((A.L.n[0] + M3_TX - 1) / M3_TX, (A.L.n[1] + M3_TY - 1) / M3_TY, (A.L.n[2] + M3_RZ - 1) / M3_RZ);
-    kern<<<grid, M3_NT, smem, s>>>(A);
+    kern<<<grid, M3_NT, smem, s>>>(A, Pol{});
     PHIX_LAUNCH_CHECK("stage_march3d");
     return PHIX_OK;
 }
@@ -214,6 +217,7 @@ struct phix_stepper {
     size_t S = 0;      // stored elements per field
     size_t esz = 8;    // element size of the state
     void* st[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    void* lo[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // FP32: low parts of the state
     bool own_state = true;
     void* kbuf[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
     int cur = 0;
@@ -242,17 +246,27 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
     make_coeffs<T>(h->phys, h->prm, A.p);
     const int c = h->cur, o = 1 - c;
     for (int f = 0; f < h->nf; ++f) A.u[f] = (const T*)h->st[c][f];
+    // compensated FP32 state: the final stage reads lo[c] and writes lo[o]
+    auto set_lo = [&](int nfl) {
+        for (int f = 0; f < nfl; ++f)
+            if (h->lo[c][f]) {
+                A.ulo[f] = (const T*)h->lo[c][f];
+                A.outlo[f] = (T*)h->lo[o][f];
+            }
+    };
     int rc;
     if (h->scheme == PHIX_MULTISTEP) {
         A.u[1] = nullptr;
         A.out[0] = (T*)h->st[o][0];
         A.mu_out = (T*)h->st[0][1];
         A.dtf = (T)h->dt;
+        set_lo(1);
         rc = launch_stage<T>(h->phys, h->dim, MODE_MULTISTEP, A, s);
         if (rc) return rc;
     } else if (h->scheme == PHIX_EULER) {
         for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->st[o][f];
         A.dtf = (T)h->dt;
+        set_lo(h->nf);
         rc = launch_stage<T>(h->phys, h->dim, MODE_EULER_FINAL, A, s);
         if (rc) return rc;
     } else {
@@ -278,6 +292,7 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
         }
         A.a = dtt;
         A.dtf = (T)(h->dt / 6.0);
+        set_lo(h->nf);
         if ((rc = launch_stage<T>(h->phys, h->dim, MODE_RK4_FINAL, A, s))) return rc;
     }
     h->cur = o;
@@ -360,6 +375,15 @@ int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precisio
             if ((e = cudaMalloc(&h->st[b][f], S * h->esz)) != cudaSuccess) return fail(e, "cudaMalloc(state)");
             if ((e = cudaMemset(h->st[b][f], 0, S * h->esz)) != cudaSuccess) return fail(e, "cudaMemset(state)");
         }
+    if (precision == PHIX_F32) {
+        // the multi-step mu is recomputed every step: no low part
+        const int nlo = scheme == PHIX_MULTISTEP ? 1 : h->nf;
+        for (int b = 0; b < 2; ++b)
+            for (int f = 0; f < nlo; ++f) {
+                if ((e = cudaMalloc(&h->lo[b][f], S * 4)) != cudaSuccess) return fail(e, "cudaMalloc(lo)");
+                if ((e = cudaMemset(h->lo[b][f], 0, S * 4)) != cudaSuccess) return fail(e, "cudaMemset(lo)");
+            }
+    }
     if (scheme == PHIX_RK4)
         for (int k = 0; k < 3; ++k)
             for (int f = 0; f < h->nf; ++f) {
@@ -386,6 +410,9 @@ int phix_stepper_destroy(phix_stepper_t* h) {
                 if (p) cudaFree(p);
     for (auto& k : h->kbuf)
         for (auto& p : k)
+            if (p) cudaFree(p);
+    for (auto& b : h->lo)
+        for (auto& p : b)
             if (p) cudaFree(p);
     if (h->stage_host) cudaFree(h->stage_host);
     if (h->partials) cudaFree(h->partials);
@@ -462,6 +489,8 @@ void* stepper_state(phix_stepper* h, int f) {
 int stepper_scheme(const phix_stepper* h) { return h->scheme; }
 void stepper_mark_mu_zero(phix_stepper* h) { h->mu_zero_pending = h->scheme == PHIX_MULTISTEP; }
 void* stepper_state_buf(phix_stepper* h, int b, int f) { return h->st[b][f]; }
+void* stepper_lo_buf(phix_stepper* h, int b, int f) { return h->lo[b][f]; }
+int stepper_cur(const phix_stepper* h) { return h->cur; }
 size_t stepper_stored(const phix_stepper* h) { return h->S; }
 int stepper_prec(const phix_stepper* h) { return h->prec; }
 int stepper_nf(const phix_stepper* h) { return h->nf; }

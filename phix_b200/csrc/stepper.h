@@ -4,8 +4,8 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
-#include "../../include/phix_b200.h"
-#include "common.cuh"
+#include "phix_b200.h"
+#include "phix/detail/common.cuh"
 
 namespace phix {
 
@@ -20,6 +20,8 @@ template <typename T> int launch_stage(int phys, int dim, int mode, const StageA
 // accessors into the opaque stepper (stepper.cu)
 void* stepper_state(phix_stepper* h, int f);
 void* stepper_state_buf(phix_stepper* h, int b, int f);
+void* stepper_lo_buf(phix_stepper* h, int b, int f);
+int stepper_cur(const phix_stepper* h);
 size_t stepper_stored(const phix_stepper* h);
 int stepper_prec(const phix_stepper* h);
 int stepper_nf(const phix_stepper* h);
@@ -34,6 +36,9 @@ double* stepper_partials(phix_stepper* h, int n);
 // FP64 <-> FP32 copies of n stored elements (convert.cu)
 int convert_f64_to_f32(float* dst, const double* src, size_t n, cudaStream_t s);
 int convert_f32_to_f64(double* dst, const float* src, size_t n, cudaStream_t s);
+// x <-> compensated float pair (hi + lo)
+int convert_f64_split(float* hi, float* lo, const double* src, size_t n, cudaStream_t s);
+int convert_pair_to_f64(double* dst, const float* hi, const float* lo, size_t n, cudaStream_t s);
 
 // diagnostics core (reduce.cu): fields in precision T, FP64 accumulation.
 template <typename T>

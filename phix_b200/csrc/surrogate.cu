@@ -25,7 +25,7 @@
 #include <new>
 #include <vector>
 
-#include "common.cuh"
+#include "phix/detail/common.cuh"
 #include "stepper.h"
 #include "tc_sm100.cuh"
 

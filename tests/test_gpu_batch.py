@@ -16,6 +16,9 @@ def small_batch(prec):
     grids, phys, prms, scheme, dt, _, fields = workloads.ch2d_batch(ninst=7, seed=11, sizes=(16, 40, 64, 96, 130))
     # one zero-flux instance and one odd-sized one, to cover the BC paths
     grids[1] = px.make_grid((40, 40), bc=(px.BC_NOFLUX,) * 6)
+    f1 = np.zeros(px.stored_shape(grids[1]))
+    f1[1, 1:41, 1:41] = 0.5 + np.random.default_rng(4).uniform(-0.05, 0.05, size=(40, 40))
+    fields[1] = f1
     grids[3] = px.make_grid((70, 37))
     g3 = grids[3]
     f3 = np.zeros(px.stored_shape(g3))
