@@ -8,8 +8,8 @@ M=1, dt=0.005, single-equation RK4 (M*lap(f'(c) - kappa*lap(c), bcs)),
 c0 = 0.5 + U[-0.01, 0.01] (seed 1).
 
 One bench "step" = one output interval: STEPS_PER_INTERVAL RK4 time steps of
-the whole field, replayed from a CUDA graph (4 fused stage launches per time
-step).  L2 is flushed (256 MiB write) between timed steps, outside the timed
+the whole field, replayed from a CUDA graph (one launch per RK4 time step:
+the four stages run in shared memory; --launch stage: one launch per stage).  L2 is flushed (256 MiB write) between timed steps, outside the timed
 events.  `value` = cell-updates/s = cells x time steps / device time.
 `e2e` runs the same interval through the C ABI with pinned HOST buffers
 (phix_stepper_run_host: H2D, advance, D2H, synchronise) inside the timed
@@ -139,6 +139,9 @@ def bench_ours(args):
     alg_bytes_step = 13 * w * cells  # RK4, one field: R u,W k1 | R u,k1 W k2 | R u,k2 W k3 | R u,k1,k2,k3 W u'
 
     st = px.Stepper(phys, scheme, prec, prm, dt, g)
+    st.set_fusion(args.launch == "step")
+    st.set_tiles(args.tiles)
+    lps = st.launches_per_step
     d_in = torch.from_numpy(fields[0]).to(dev)
     st.load([d_in])
     st.set_graph(STEPS_PER_INTERVAL)
@@ -175,8 +178,8 @@ def bench_ours(args):
     ms_per_step = total_ms / args.steps
     value = world * cells * STEPS_PER_INTERVAL * args.steps / (total_ms / 1e3)
 
-    # roofline of the fused stage kernels: algorithmic bytes of one time step
-    # (4 launches) over the device time of one time step
+    # roofline: algorithmic bytes of one time step (13w per cell, the traffic
+    # of one launch per stage) over the device time of one time step
     t_timestep = ms_per_step / 1e3 / STEPS_PER_INTERVAL
     achieved = alg_bytes_step / t_timestep / 1e9
     peak, peak_kind = _peaks()
@@ -243,13 +246,15 @@ def bench_ours(args):
             "dtype": args.dtype,
             "data": DATA,
             "config": {"workload": WORKLOAD, "cells": cells, "time_steps_per_step": STEPS_PER_INTERVAL,
+                       "launches_per_time_step": lps,
                        "precision_note": "FP64 stencils" if prec == px.F64 else "FP32 stencils, FP64 reductions",
                        "l2": "flushed between timed steps (256 MiB write); one step keeps its field L2-resident",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
-                         "note": f"algorithmic {13 * w} B/cell-update (13w RK4) over CUDA-event time of the "
-                                 f"4 fused stage launches per time step; peak {peak_kind}"},
+                         "note": f"algorithmic {13 * w} B/cell-update (13w RK4) over the CUDA-event time of "
+                                 f"one time step ({lps} launch{'es' if lps > 1 else ''} per time step); "
+                                 f"peak {peak_kind}"},
             "hbm_gbs_effective": achieved,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": stored_bytes,
@@ -338,6 +343,9 @@ def main():
     ap.add_argument("--n", type=int, default=1024, help="grid size n x n (the metric is quoted at 1024)")
     ap.add_argument("--cpu-baseline-steps", type=int, default=50)
     ap.add_argument("--ref-sample-steps", type=int, default=2)
+    ap.add_argument("--tiles", type=int, default=-1, help="2-D stage tile shape (phix_stepper_set_tiles)")
+    ap.add_argument("--launch", choices=["step", "stage"], default="step",
+                    help="one launch per RK4 time step (default) or one per stage")
     args = ap.parse_args()
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)  # timing rule: at least 3 untimed warm-up steps

@@ -218,6 +218,31 @@ __device__ __forceinline__ void write_ghost(const StageArgs<T>& A, int nf, int p
     }
 }
 
+// Ghost layers of the new state next to the TX x TY tile at (x0, y0): the
+// final stage writes them so the new state's stored array is complete.
+template <typename T, int DIM, int NF, int TX, int TY, int NT>
+__device__ __forceinline__ void box_ghosts(const StageArgs<T>& A, int x0, int y0) {
+    const int n0 = A.L.n[0], n1 = A.L.n[1], gl = A.L.ghost;
+    // x faces
+    if (x0 == 0 || x0 + TX >= n0) {
+        for (int i = threadIdx.x; i < TY * gl; i += NT) {
+            const int py = y0 + i / gl, l = 1 + i % gl;
+            if (DIM >= 2 && py >= n1) continue;
+            if (DIM < 2 && i / gl > 0) continue;
+            if (x0 == 0) write_ghost<T, DIM>(A, NF, -l, DIM >= 2 ? py : 0, 0);
+            if (x0 + TX >= n0) write_ghost<T, DIM>(A, NF, n0 - 1 + l, DIM >= 2 ? py : 0, 0);
+        }
+    }
+    if (DIM >= 2 && (y0 == 0 || y0 + TY >= n1)) {
+        for (int i = threadIdx.x; i < TX * gl; i += NT) {
+            const int px = x0 + i % TX, l = 1 + i / TX;
+            if (px >= n0) continue;
+            if (y0 == 0) write_ghost<T, DIM>(A, NF, px, -l, 0);
+            if (y0 + TY >= n1) write_ghost<T, DIM>(A, NF, px, n1 - 1 + l, 0);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // 1-D / 2-D: box tile
 // ---------------------------------------------------------------------------
@@ -311,6 +336,7 @@ __device__ __forceinline__ void box_tile(const StageArgs<T>& A, const Pol& pol, 
         for (int i = threadIdx.x; i < MX * MY; i += NT) {
             const int lx = i % MX, ly = i / MX;
             const int px = x0 - 1 + lx, py = y0 - (DIM >= 2 ? 1 : 0) + ly;
+            if (px < -1 || px > n0 || (DIM >= 2 && (py < -1 || py > n1))) continue;  // past ghost layer 1
             const bool outx = px < 0 || px >= n0, outy = DIM >= 2 && (py < 0 || py >= n1);
             if (outx == outy) continue;  // interior or corner
             if (outx && (py < y0 || py >= y0 + TY)) continue;  // owned by the neighbour tile row
@@ -320,27 +346,7 @@ __device__ __forceinline__ void box_tile(const StageArgs<T>& A, const Pol& pol, 
         }
     }
 
-    if (MODE != MODE_K && !interior) {
-        const int gl = A.L.ghost;
-        // x faces
-        if (x0 == 0 || x0 + TX >= n0) {
-            for (int i = threadIdx.x; i < TY * gl; i += NT) {
-                const int py = y0 + i / gl, l = 1 + i % gl;
-                if (DIM >= 2 && py >= n1) continue;
-                if (DIM < 2 && i / gl > 0) continue;
-                if (x0 == 0) write_ghost<T, DIM>(A, NF, -l, DIM >= 2 ? py : 0, 0);
-                if (x0 + TX >= n0) write_ghost<T, DIM>(A, NF, n0 - 1 + l, DIM >= 2 ? py : 0, 0);
-            }
-        }
-        if (DIM >= 2 && (y0 == 0 || y0 + TY >= n1)) {
-            for (int i = threadIdx.x; i < TX * gl; i += NT) {
-                const int px = x0 + i % TX, l = 1 + i / TX;
-                if (px >= n0) continue;
-                if (y0 == 0) write_ghost<T, DIM>(A, NF, px, -l, 0);
-                if (y0 + TY >= n1) write_ghost<T, DIM>(A, NF, px, n1 - 1 + l, 0);
-            }
-        }
-    }
+    if (MODE != MODE_K && !interior) box_ghosts<T, DIM, NF, TX, TY, NT>(A, x0, y0);
 }
 
 // Single field: one CTA per tile.

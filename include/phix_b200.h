@@ -144,7 +144,9 @@ int phix_stepper_store(phix_stepper_t* h, double* const* fields, void* stream);
 
 /* Advance nsteps time steps on `stream`.  Each step is one launch per RK
  * stage (4 for RK4, 1 for Euler) with the BCs, the stage combination and the
- * final update fused in.  When steps_per_graph > 0 (see
+ * final update fused in; a single-field 2-D RK4 step whose sides are all
+ * periodic or zero-flux is one launch for all four stages (see
+ * phix_stepper_set_fusion).  When steps_per_graph > 0 (see
  * phix_stepper_set_graph) whole groups of steps replay as one CUDA graph.
  * Replaces Solver::advance / VectorSolver::advance (Solver.cu:366-382). */
 int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream);
@@ -153,6 +155,21 @@ int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream);
  * (0 disables graphs).  Replaces the driver step loop (Solver::run,
  * Solver.cu:405-414) between callbacks. */
 int phix_stepper_set_graph(phix_stepper_t* h, int steps_per_graph);
+
+/* 1 (default): where supported, run each RK4 step as one launch that keeps
+ * the four stage states in shared memory and recomputes the tile halos;
+ * 0: one launch per stage.  Both give the same bits.  No reference
+ * counterpart (the reference runs each term and stage as its own kernels). */
+int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step);
+
+/* Kernel launches one time step takes with the current settings. */
+int phix_stepper_launches_per_step(const phix_stepper_t* h);
+
+/* Tile shape of the 2-D per-stage kernels: -1 (default) the box tiles (64x16,
+ * 256 threads), 0..3 column-walking tiles (TX x TY = 128x16, 64x16, 64x32,
+ * 128x32; one thread per column).  All give the same bits.  No reference
+ * counterpart. */
+int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg);
 
 /* FP64 only: run directly on caller-owned buffers, no copies.  fields[f] is
  * the current state and alt[f] a second stored array of the same size.

@@ -281,3 +281,8 @@ def build(with_ref: bool | None = None, quiet: bool = True) -> None:
         with_ref = os.path.isdir(os.path.join(ref_src, "src"))
     if with_ref:
         subprocess.run(["make", "-C", HERE, "-j8", "ref", f"REF={ref_src}"], check=True, stdout=out)
+        cxx = os.path.join(os.path.dirname(HERE), "phix_b200", "libphix_cxx.so")
+        if os.path.exists(cxx):
+            from phix_b200.build import json_include
+            subprocess.run(["make", "-C", HERE, "-j4", "dropin", f"REF={ref_src}", f"JSON_INC={json_include() or ''}"],
+                           check=True, stdout=out)

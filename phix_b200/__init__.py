@@ -104,6 +104,9 @@ def lib() -> C.CDLL:
         "phix_stepper_store": ([vp, C.POINTER(vp), vp], C.c_int),
         "phix_stepper_advance": ([vp, C.c_int, vp], C.c_int),
         "phix_stepper_set_graph": ([vp, C.c_int], C.c_int),
+        "phix_stepper_set_fusion": ([vp, C.c_int], C.c_int),
+        "phix_stepper_launches_per_step": ([vp], C.c_int),
+        "phix_stepper_set_tiles": ([vp, C.c_int], C.c_int),
         "phix_stepper_bind": ([vp, C.POINTER(vp), C.POINTER(vp)], C.c_int),
         "phix_stepper_current": ([vp], C.c_int),
         "phix_stepper_run_host": ([vp, C.POINTER(vp), C.POINTER(vp), C.c_int], C.c_int),
@@ -255,6 +258,18 @@ class Stepper:
 
     def set_graph(self, steps_per_graph: int):
         check(lib().phix_stepper_set_graph(self.h, steps_per_graph))
+
+    def set_fusion(self, on: bool):
+        """One launch per RK4 step (True, default where supported) or per stage."""
+        check(lib().phix_stepper_set_fusion(self.h, 1 if on else 0))
+
+    @property
+    def launches_per_step(self) -> int:
+        return lib().phix_stepper_launches_per_step(self.h)
+
+    def set_tiles(self, cfg: int):
+        """2-D stage tile shape (0..3 column-walking tiles, -1 generic box tiles)."""
+        check(lib().phix_stepper_set_tiles(self.h, cfg))
 
     def bind(self, fields, alt):
         check(lib().phix_stepper_bind(self.h, _ptrs(fields), _ptrs(alt)))

@@ -112,7 +112,7 @@ int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s
             }
         }
     }
-    stepper_mark_mu_zero(h);
+    stepper_mark_loaded(h);
     return PHIX_OK;
 }
 

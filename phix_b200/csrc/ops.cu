@@ -81,8 +81,12 @@ __global__ void __launch_bounds__(256) k_axpy(double* __restrict__ dst, const do
 
 // One BC object's ghost fill over the full stored extent of the other two
 // axes (ghost corners included, every layer), as in Boundary.cu:95-195.
-__global__ void __launch_bounds__(256) k_bc_face(double* __restrict__ data, Layout L, int axis, int type, int do_lo,
-                                                 int do_hi, double v_lo, double v_hi) {
+// `low_part`: data is the low part of a compensated state (Dirichlet ghosts
+// get 0, their value lives in the high part).
+template <typename T>
+__global__ void __launch_bounds__(256) k_bc_face(T* __restrict__ data, Layout L, int axis, int type, int do_lo,
+                                                 int do_hi, double v_lo, double v_hi, int low_part) {
+    if (low_part) v_lo = v_hi = 0.0;
     const int sx = L.s[1], sy = L.s[2] / L.s[1], sz = L.n[2] + 2 * L.ghost;
     int nf0, nf1, fs0, fs1, astr;
     if (axis == 0) { astr = 1; nf0 = sy; nf1 = sz; fs0 = sx; fs1 = sx * sy; }
@@ -102,8 +106,8 @@ __global__ void __launch_bounds__(256) k_bc_face(double* __restrict__ data, Layo
                 if (do_lo) data[lo] = data[g * astr + off];
                 if (do_hi) data[hi] = data[(g + n - 1) * astr + off];
             } else {
-                if (do_lo) data[lo] = v_lo;
-                if (do_hi) data[hi] = v_hi;
+                if (do_lo) data[lo] = (T)v_lo;
+                if (do_hi) data[hi] = (T)v_hi;
             }
         }
     }
@@ -119,27 +123,24 @@ void inv_d2(const phix_grid_t* g, double* i2) {
 }
 
 }  // namespace
-}  // namespace phix
 
-using namespace phix;
-
-extern "C" {
-
-int phix_bc_apply(double* field, const phix_grid_t* g, void* stream) {
+// Every BC of the grid, in buildBCs order (BCFactory.cpp:50-74): axis x, y, z;
+// a periodic axis is one BC object, otherwise the LOW then the HIGH side.
+template <typename T>
+int bc_fill(T* field, const phix_grid_t* g, bool low_part, cudaStream_t s) {
     Layout L;
     int rc = validate_grid(g, &L, nullptr);
-    if (rc || (rc = check_ptrs(field))) return rc;
-    cudaStream_t s = (cudaStream_t)stream;
+    if (rc) return rc;
     auto launch = [&](int axis, int type, int lo, int hi) -> int {
         const int sx = L.s[1], sy = L.s[2] / L.s[1], sz = L.n[2] + 2 * L.ghost;
         long long faces = axis == 0 ? (long long)sy * sz : axis == 1 ? (long long)sx * sz : (long long)sx * sy;
         int blocks = (int)((faces + 255) / 256);
         if (blocks > 148 * 8) blocks = 148 * 8;
-        k_bc_face<<<blocks, 256, 0, s>>>(field, L, axis, type, lo, hi, g->bc_val[2 * axis], g->bc_val[2 * axis + 1]);
+        k_bc_face<T><<<blocks, 256, 0, s>>>(field, L, axis, type, lo, hi, g->bc_val[2 * axis], g->bc_val[2 * axis + 1],
+                                            low_part ? 1 : 0);
         PHIX_LAUNCH_CHECK("k_bc_face");
         return PHIX_OK;
     };
-    // buildBCs order (BCFactory.cpp:50-74)
     for (int a = 0; a < g->dim; ++a) {
         const int tl = g->bc_type[2 * a], th = g->bc_type[2 * a + 1];
         if (tl == PHIX_BC_PERIODIC) {
@@ -152,6 +153,20 @@ int phix_bc_apply(double* field, const phix_grid_t* g, void* stream) {
             if ((rc = launch(a, th, 0, 1))) return rc;
     }
     return PHIX_OK;
+}
+template int bc_fill<float>(float*, const phix_grid_t*, bool, cudaStream_t);
+template int bc_fill<double>(double*, const phix_grid_t*, bool, cudaStream_t);
+
+}  // namespace phix
+
+using namespace phix;
+
+extern "C" {
+
+int phix_bc_apply(double* field, const phix_grid_t* g, void* stream) {
+    int rc = validate_grid(g, nullptr, nullptr);
+    if (rc || (rc = check_ptrs(field))) return rc;
+    return bc_fill<double>(field, g, false, (cudaStream_t)stream);
 }
 
 int phix_lap_accumulate(double* rhs, const double* src, double coeff, const phix_grid_t* g, void* stream) {

@@ -16,6 +16,8 @@
 
 #include "phix/detail/common.cuh"
 #include "phix/detail/stage.cuh"
+#include "phix/detail/stage_col.cuh"
+#include "phix/detail/step2d.cuh"
 #include "stepper.h"
 
 namespace phix {
@@ -29,9 +31,48 @@ constexpr int BOX_TX = 64, BOX_TY = 16, BOX_NT = 256;
 constexpr int LIN_TX = 256, LIN_NT = 256;
 constexpr int M3_TX = 32, M3_TY = 8, M3_RZ = 16, M3_NT = 256;
 
+// 2-D column-walking tiles (stage_col.cuh): (TX, TY) per configuration.
+constexpr int kColCfgs[][2] = {{128, 16}, {64, 16}, {64, 32}, {128, 32}};
+constexpr int kNumColCfgs = sizeof(kColCfgs) / sizeof(kColCfgs[0]);
+
+template <typename T, class Pol, int MODE, int TX, int TY>
+int launch_col_cfg(const StageArgs<T>& A, cudaStream_t s) {
+    dim3 grid((A.L.n[0] + TX - 1) / TX, (A.L.n[1] + TY - 1) / TY, 1);
+    stage_col<T, Pol, MODE, TX, TY><<<grid, TX, col_smem_bytes<T, Pol, TX, TY>(), s>>>(A, Pol{});
+    PHIX_LAUNCH_CHECK("stage_col");
+    return PHIX_OK;
+}
+
+template <typename T, class Pol, int MODE, int TX, int TY>
+int prepare_col_cfg() {
+    PHIX_TRY_CUDA(cudaFuncSetAttribute(stage_col<T, Pol, MODE, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)col_smem_bytes<T, Pol, TX, TY>()));
+    return PHIX_OK;
+}
+
+template <typename T, class Pol, int MODE>
+int col_dispatch(int cfg, bool prepare, const StageArgs<T>* A, cudaStream_t s) {
+    switch (cfg) {
+#define PHIX_COL_CASE(i)                                                                         \
+    case i:                                                                                      \
+        return prepare ? prepare_col_cfg<T, Pol, MODE, kColCfgs[i][0], kColCfgs[i][1]>()         \
+                       : launch_col_cfg<T, Pol, MODE, kColCfgs[i][0], kColCfgs[i][1]>(*A, s);
+        PHIX_COL_CASE(0)
+        PHIX_COL_CASE(1)
+        PHIX_COL_CASE(2)
+        PHIX_COL_CASE(3)
+#undef PHIX_COL_CASE
+    }
+    set_error("stage: bad 2-D tile configuration %d", cfg);
+    return PHIX_ERR_ARG;
+}
+
 template <typename T, int PHYS, int DIM, int MODE>
-int launch_box(const StageArgs<T>& A, cudaStream_t s) {
+int launch_box(const StageArgs<T>& A, cudaStream_t s, int tile) {
     using Pol = typename PolOf<PHYS>::type;
+    if constexpr (DIM == 2 && MODE != MODE_MULTISTEP) {
+        if (tile >= 0) return col_dispatch<T, Pol, MODE>(tile, false, &A, s);
+    }
     if (DIM == 1) {
         dim3 grid((A.L.n[0] + LIN_TX - 1) / LIN_TX, 1, 1);
         stage_box<T, Pol, 1, MODE, LIN_TX, 1, LIN_NT><<<grid, LIN_NT, 0, s>>>(A, Pol{});
@@ -84,10 +125,10 @@ int launch_march(const StageArgs<T>& A, cudaStream_t s) {
 }
 
 template <typename T, int PHYS, int MODE>
-int launch_dim(int dim, const StageArgs<T>& A, cudaStream_t s) {
+int launch_dim(int dim, const StageArgs<T>& A, cudaStream_t s, int tile) {
     switch (dim) {
-        case 1: return launch_box<T, PHYS, 1, MODE>(A, s);
-        case 2: return launch_box<T, PHYS, 2, MODE>(A, s);
+        case 1: return launch_box<T, PHYS, 1, MODE>(A, s, tile);
+        case 2: return launch_box<T, PHYS, 2, MODE>(A, s, tile);
         case 3: return launch_march<T, PHYS, MODE>(A, s);
     }
     set_error("stage: unsupported dim %d", dim);
@@ -95,15 +136,15 @@ int launch_dim(int dim, const StageArgs<T>& A, cudaStream_t s) {
 }
 
 template <typename T, int PHYS>
-int launch_mode(int dim, int mode, const StageArgs<T>& A, cudaStream_t s) {
+int launch_mode(int dim, int mode, const StageArgs<T>& A, cudaStream_t s, int tile) {
     switch (mode) {
-        case MODE_K: return launch_dim<T, PHYS, MODE_K>(dim, A, s);
-        case MODE_RK4_FINAL: return launch_dim<T, PHYS, MODE_RK4_FINAL>(dim, A, s);
-        case MODE_EULER_FINAL: return launch_dim<T, PHYS, MODE_EULER_FINAL>(dim, A, s);
+        case MODE_K: return launch_dim<T, PHYS, MODE_K>(dim, A, s, tile);
+        case MODE_RK4_FINAL: return launch_dim<T, PHYS, MODE_RK4_FINAL>(dim, A, s, tile);
+        case MODE_EULER_FINAL: return launch_dim<T, PHYS, MODE_EULER_FINAL>(dim, A, s, tile);
         case MODE_MULTISTEP:
             if (PHYS == PHIX_PHYS_CH && dim <= 2) {
-                if (dim == 1) return launch_box<T, PHIX_PHYS_CH, 1, MODE_MULTISTEP>(A, s);
-                return launch_box<T, PHIX_PHYS_CH, 2, MODE_MULTISTEP>(A, s);
+                if (dim == 1) return launch_box<T, PHIX_PHYS_CH, 1, MODE_MULTISTEP>(A, s, -1);
+                return launch_box<T, PHIX_PHYS_CH, 2, MODE_MULTISTEP>(A, s, -1);
             }
             break;
     }
@@ -111,25 +152,88 @@ int launch_mode(int dim, int mode, const StageArgs<T>& A, cudaStream_t s) {
     return PHIX_ERR_ARG;
 }
 
+// ---------------------------------------------------------------------------
+// one launch per RK4 step (2-D, one field)
+// ---------------------------------------------------------------------------
+constexpr int ST_TX = 64, ST_TY = 16, ST_NT = 256;
+
+template <typename T, int PHYS>
+int prepare_step2d_t() {
+    using Pol = typename PolOf<PHYS>::type;
+    using G = Step2D<T, Pol, ST_TX, ST_TY>;
+    PHIX_TRY_CUDA(cudaFuncSetAttribute(step_box<T, Pol, ST_TX, ST_TY, ST_NT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
+    return PHIX_OK;
+}
+
+template <typename T, int PHYS>
+int launch_step2d_t(const StepArgs<T>& A, cudaStream_t s) {
+    using Pol = typename PolOf<PHYS>::type;
+    using G = Step2D<T, Pol, ST_TX, ST_TY>;
+    dim3 grid((A.S.L.n[0] + ST_TX - 1) / ST_TX, (A.S.L.n[1] + ST_TY - 1) / ST_TY, 1);
+    step_box<T, Pol, ST_TX, ST_TY, ST_NT><<<grid, ST_NT, G::smem_bytes(), s>>>(A, Pol{});
+    PHIX_LAUNCH_CHECK("step_box");
+    return PHIX_OK;
+}
+
 }  // namespace
 
+template <typename T, int PHYS>
+int prepare_col_t() {
+    using Pol = typename PolOf<PHYS>::type;
+    for (int c = 0; c < kNumColCfgs; ++c) {
+        int rc;
+        if ((rc = col_dispatch<T, Pol, MODE_K>(c, true, nullptr, 0))) return rc;
+        if ((rc = col_dispatch<T, Pol, MODE_RK4_FINAL>(c, true, nullptr, 0))) return rc;
+        if ((rc = col_dispatch<T, Pol, MODE_EULER_FINAL>(c, true, nullptr, 0))) return rc;
+    }
+    return PHIX_OK;
+}
+
 int prepare_stage(int phys, int dim, int prec) {
+    if (dim == 2) {
+        int rc;
+        if (prec == PHIX_F32)
+            rc = phys == PHIX_PHYS_AC ? prepare_col_t<float, PHIX_PHYS_AC>()
+               : phys == PHIX_PHYS_CH ? prepare_col_t<float, PHIX_PHYS_CH>() : prepare_col_t<float, PHIX_PHYS_CHAC>();
+        else
+            rc = phys == PHIX_PHYS_AC ? prepare_col_t<double, PHIX_PHYS_AC>()
+               : phys == PHIX_PHYS_CH ? prepare_col_t<double, PHIX_PHYS_CH>() : prepare_col_t<double, PHIX_PHYS_CHAC>();
+        if (rc) return rc;
+    }
+    if (dim == 2 && (phys == PHIX_PHYS_AC || phys == PHIX_PHYS_CH)) {
+        int rc;
+        if (prec == PHIX_F32)
+            rc = phys == PHIX_PHYS_AC ? prepare_step2d_t<float, PHIX_PHYS_AC>() : prepare_step2d_t<float, PHIX_PHYS_CH>();
+        else
+            rc = phys == PHIX_PHYS_AC ? prepare_step2d_t<double, PHIX_PHYS_AC>()
+                                      : prepare_step2d_t<double, PHIX_PHYS_CH>();
+        if (rc) return rc;
+    }
     if (dim != 3) return PHIX_OK;
     return prec == PHIX_F32 ? prepare_t<float>(phys) : prepare_t<double>(phys);
 }
 
 template <typename T>
-int launch_stage(int phys, int dim, int mode, const StageArgs<T>& A, cudaStream_t s) {
+int launch_step2d(int phys, const StepArgs<T>& A, cudaStream_t s) {
+    if (phys == PHIX_PHYS_AC) return launch_step2d_t<T, PHIX_PHYS_AC>(A, s);
+    if (phys == PHIX_PHYS_CH) return launch_step2d_t<T, PHIX_PHYS_CH>(A, s);
+    set_error("step2d: physics %d has more than one field", phys);
+    return PHIX_ERR_UNSUPPORTED;
+}
+
+template <typename T>
+int launch_stage(int phys, int dim, int mode, const StageArgs<T>& A, cudaStream_t s, int tile) {
     switch (phys) {
-        case PHIX_PHYS_AC: return launch_mode<T, PHIX_PHYS_AC>(dim, mode, A, s);
-        case PHIX_PHYS_CH: return launch_mode<T, PHIX_PHYS_CH>(dim, mode, A, s);
-        case PHIX_PHYS_CHAC: return launch_mode<T, PHIX_PHYS_CHAC>(dim, mode, A, s);
+        case PHIX_PHYS_AC: return launch_mode<T, PHIX_PHYS_AC>(dim, mode, A, s, tile);
+        case PHIX_PHYS_CH: return launch_mode<T, PHIX_PHYS_CH>(dim, mode, A, s, tile);
+        case PHIX_PHYS_CHAC: return launch_mode<T, PHIX_PHYS_CHAC>(dim, mode, A, s, tile);
     }
     set_error("stage: unknown physics %d", phys);
     return PHIX_ERR_ARG;
 }
-template int launch_stage<float>(int, int, int, const StageArgs<float>&, cudaStream_t);
-template int launch_stage<double>(int, int, int, const StageArgs<double>&, cudaStream_t);
+template int launch_stage<float>(int, int, int, const StageArgs<float>&, cudaStream_t, int);
+template int launch_stage<double>(int, int, int, const StageArgs<double>&, cudaStream_t, int);
 
 // ---------------------------------------------------------------------------
 // grid validation / layout
@@ -222,6 +326,13 @@ struct phix_stepper {
     void* kbuf[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
     int cur = 0;
     bool mu_zero_pending = false;  // MULTISTEP: the STEADY field is zeroed by its first evaluation
+    // The first step of a loaded state applies every BC to the whole stored
+    // arrays (as the reference's step does), which also fills the ghost cells
+    // of padding planes; the fused kernels keep the physical plane's ghosts
+    // current from then on.
+    bool bc_pending = false;
+    bool fuse_steps = true;  // one launch per RK4 step where step2d supports the grid
+    int tile = -1;           // 2-D stage tiles: -1 generic box tiles (fastest measured), else kColCfgs index
     cudaStream_t cap = nullptr;
     int graph_steps = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -235,6 +346,14 @@ namespace phix {
 static void drop_graphs(phix_stepper* h) {
     for (auto& e : h->gexec)
         if (e) { cudaGraphExecDestroy(e); e = nullptr; }
+}
+
+static bool step_fused(const phix_stepper* h) {
+    return h->fuse_steps && h->scheme == PHIX_RK4 && h->nf == 1 && step2d_supported(h->L, h->dim);
+}
+
+static int launches_per_step(const phix_stepper* h) {
+    return h->scheme == PHIX_RK4 && !step_fused(h) ? 4 : 1;
 }
 
 template <typename T>
@@ -261,19 +380,28 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
         A.mu_out = (T*)h->st[0][1];
         A.dtf = (T)h->dt;
         set_lo(1);
-        rc = launch_stage<T>(h->phys, h->dim, MODE_MULTISTEP, A, s);
+        rc = launch_stage<T>(h->phys, h->dim, MODE_MULTISTEP, A, s, h->tile);
         if (rc) return rc;
     } else if (h->scheme == PHIX_EULER) {
         for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->st[o][f];
         A.dtf = (T)h->dt;
         set_lo(h->nf);
-        rc = launch_stage<T>(h->phys, h->dim, MODE_EULER_FINAL, A, s);
+        rc = launch_stage<T>(h->phys, h->dim, MODE_EULER_FINAL, A, s, h->tile);
         if (rc) return rc;
+    } else if (step_fused(h)) {
+        A.out[0] = (T*)h->st[o][0];
+        A.dtf = (T)(h->dt / 6.0);
+        set_lo(1);
+        StepArgs<T> B;
+        B.S = A;
+        B.dt2 = (T)(h->dt * 0.5);
+        B.dt = (T)h->dt;
+        if ((rc = launch_step2d<T>(h->phys, B, s))) return rc;
     } else {
         const T dt2 = (T)(h->dt * 0.5), dtt = (T)h->dt;
         // stage 1
         for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->kbuf[0][f];
-        if ((rc = launch_stage<T>(h->phys, h->dim, MODE_K, A, s))) return rc;
+        if ((rc = launch_stage<T>(h->phys, h->dim, MODE_K, A, s, h->tile))) return rc;
         // stages 2, 3
         for (int st = 1; st < 3; ++st) {
             for (int f = 0; f < h->nf; ++f) {
@@ -281,7 +409,7 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
                 A.out[f] = (T*)h->kbuf[st][f];
             }
             A.a = dt2;
-            if ((rc = launch_stage<T>(h->phys, h->dim, MODE_K, A, s))) return rc;
+            if ((rc = launch_stage<T>(h->phys, h->dim, MODE_K, A, s, h->tile))) return rc;
         }
         // stage 4 + update
         for (int f = 0; f < h->nf; ++f) {
@@ -293,7 +421,7 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
         A.a = dtt;
         A.dtf = (T)(h->dt / 6.0);
         set_lo(h->nf);
-        if ((rc = launch_stage<T>(h->phys, h->dim, MODE_RK4_FINAL, A, s))) return rc;
+        if ((rc = launch_stage<T>(h->phys, h->dim, MODE_RK4_FINAL, A, s, h->tile))) return rc;
     }
     h->cur = o;
     return PHIX_OK;
@@ -323,7 +451,7 @@ static int replay_group(phix_stepper* h, cudaStream_t s) {
     }
     PHIX_TRY_CUDA(cudaGraphLaunch(h->gexec[parity], s));
     // launches inside the graph count as kernel launches of this library
-    count_launch(h->graph_steps * (h->scheme == PHIX_RK4 ? 4 : 1));
+    count_launch(h->graph_steps * launches_per_step(h));
     if (h->graph_steps % 2) h->cur = 1 - parity;
     return PHIX_OK;
 }
@@ -432,6 +560,27 @@ int phix_stepper_set_graph(phix_stepper_t* h, int steps_per_graph) {
     return PHIX_OK;
 }
 
+int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step) {
+    if (!h) { set_error("set_fusion: NULL stepper"); return PHIX_ERR_ARG; }
+    const bool f = one_launch_per_step != 0;
+    if (f != h->fuse_steps) {
+        drop_graphs(h);
+        h->fuse_steps = f;
+    }
+    return PHIX_OK;
+}
+
+int phix_stepper_launches_per_step(const phix_stepper_t* h) { return h ? launches_per_step(h) : -1; }
+
+int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg) {
+    if (!h || tile_cfg < -1 || tile_cfg >= kNumColCfgs) { set_error("set_tiles: bad stepper or configuration"); return PHIX_ERR_ARG; }
+    if (tile_cfg != h->tile) {
+        drop_graphs(h);
+        h->tile = tile_cfg;
+    }
+    return PHIX_OK;
+}
+
 int phix_stepper_bind(phix_stepper_t* h, double* const* fields, double* const* alt) {
     if (!h || !fields || !alt) { set_error("bind: NULL argument"); return PHIX_ERR_ARG; }
     if (h->prec != PHIX_F64) { set_error("bind: only FP64 steppers run on caller buffers"); return PHIX_ERR_UNSUPPORTED; }
@@ -454,6 +603,7 @@ int phix_stepper_bind(phix_stepper_t* h, double* const* fields, double* const* a
     }
     h->cur = 0;
     h->mu_zero_pending = h->scheme == PHIX_MULTISTEP;
+    h->bc_pending = true;
     return PHIX_OK;
 }
 
@@ -465,6 +615,16 @@ int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream) {
     if (h->mu_zero_pending && nsteps > 0) {
         PHIX_TRY_CUDA(cudaMemsetAsync(h->st[0][1], 0, h->S * h->esz, s));
         h->mu_zero_pending = false;
+    }
+    if (h->bc_pending && nsteps > 0) {
+        for (int f = 0; f < h->nf; ++f)
+            for (int b = 0; b < (h->scheme == PHIX_MULTISTEP && f == 1 ? 1 : 2); ++b) {  // one mu buffer
+                if (h->prec == PHIX_F64) rc = bc_fill<double>((double*)h->st[b][f], &h->g, false, s);
+                else rc = bc_fill<float>((float*)h->st[b][f], &h->g, false, s);
+                if (rc) return rc;
+                if (h->lo[b][f] && (rc = bc_fill<float>((float*)h->lo[b][f], &h->g, true, s))) return rc;
+            }
+        h->bc_pending = false;
     }
     if (h->graph_steps > 0) {
         while (nsteps >= h->graph_steps) {
@@ -487,7 +647,10 @@ void* stepper_state(phix_stepper* h, int f) {
     return h->st[h->cur][f];
 }
 int stepper_scheme(const phix_stepper* h) { return h->scheme; }
-void stepper_mark_mu_zero(phix_stepper* h) { h->mu_zero_pending = h->scheme == PHIX_MULTISTEP; }
+void stepper_mark_loaded(phix_stepper* h) {
+    h->mu_zero_pending = h->scheme == PHIX_MULTISTEP;
+    h->bc_pending = true;
+}
 void* stepper_state_buf(phix_stepper* h, int b, int f) { return h->st[b][f]; }
 void* stepper_lo_buf(phix_stepper* h, int b, int f) { return h->lo[b][f]; }
 int stepper_cur(const phix_stepper* h) { return h->cur; }

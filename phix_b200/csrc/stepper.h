@@ -15,7 +15,7 @@ int validate_grid(const phix_grid_t* g, Layout* L, size_t* stored);
 int physics_nfields(int phys);
 template <typename T> void make_coeffs(int phys, const double* prm, T* p);
 int prepare_stage(int phys, int dim, int prec);
-template <typename T> int launch_stage(int phys, int dim, int mode, const StageArgs<T>& A, cudaStream_t s);
+template <typename T> int launch_stage(int phys, int dim, int mode, const StageArgs<T>& A, cudaStream_t s, int tile = -1);
 
 // accessors into the opaque stepper (stepper.cu)
 void* stepper_state(phix_stepper* h, int f);
@@ -27,11 +27,15 @@ int stepper_prec(const phix_stepper* h);
 int stepper_nf(const phix_stepper* h);
 int stepper_phys(const phix_stepper* h);
 int stepper_scheme(const phix_stepper* h);
-void stepper_mark_mu_zero(phix_stepper* h);
+void stepper_mark_loaded(phix_stepper* h);
 const phix_grid_t* stepper_grid(const phix_stepper* h);
 const double* stepper_prm(const phix_stepper* h);
 double* stepper_staging(phix_stepper* h);
 double* stepper_partials(phix_stepper* h, int n);
+
+// All BCs of g applied to a stored array (ops.cu); low_part: the array is the
+// low part of a compensated state.
+template <typename T> int bc_fill(T* field, const phix_grid_t* g, bool low_part, cudaStream_t s);
 
 // FP64 <-> FP32 copies of n stored elements (convert.cu)
 int convert_f64_to_f32(float* dst, const double* src, size_t n, cudaStream_t s);

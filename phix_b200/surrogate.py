@@ -58,10 +58,8 @@ def train(seeds, nsteps: int = 40000, every: int = STEPS_PER_CALL, batch: int = 
     """Train on FD trajectories generated on the fly; returns (flat params, log)."""
     import torch
 
-    from oracle import surrogate_oracle as _so  # noqa: F401  (only for init shapes)
-    from . import surrogate_params_to_flat
     if params is None:
-        params = surrogate_params_to_flat(_init_params(init_seed))
+        params = init_params(init_seed)
     sg = Surrogate(n, n, batch, IN_SHIFT, IN_SCALE, OUT_SCALE)
     sg.set_params(params)
     log = TrainLog()
@@ -107,9 +105,21 @@ def train(seeds, nsteps: int = 40000, every: int = STEPS_PER_CALL, batch: int = 
     return p, log
 
 
-def _init_params(seed):
-    from oracle import surrogate_oracle as so
-    return so.init_params(seed)
+LAYERS = ((1, 32), (32, 32), (32, 32), (32, 1))
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-normal weights (std sqrt(2 / (9 cin))), zero biases, the last layer
+    scaled by 0.1 so the untrained step is close to the identity; returned as
+    the flat FP32 vector of phix_surrogate_set_params (W[cout, ky, kx, cin])."""
+    from . import surrogate_params_to_flat
+    rng = np.random.default_rng(seed)
+    params = []
+    for cin, cout in LAYERS:
+        w = rng.normal(0.0, np.sqrt(2.0 / (9 * cin)), size=(cout, 3, 3, cin)).astype(np.float32)
+        params += [w, np.zeros(cout, dtype=np.float32)]
+    params[6] *= 0.1
+    return surrogate_params_to_flat(params)
 
 
 def fd_run(c0: np.ndarray, nsteps: int, precision=F64, graph: int = 100):

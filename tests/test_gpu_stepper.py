@@ -56,6 +56,13 @@ def corner_mask(grid):
     return out >= 2
 
 
+def _where(a, b, keep):
+    """First mismatching stored cells (z, y, x): got / want."""
+    bad = np.argwhere((a != b) & keep)
+    return f"{len(bad)} cells differ, first: " + ", ".join(
+        f"{tuple(int(v) for v in i)} {a[tuple(i)]:.6g}/{b[tuple(i)]:.6g}" for i in bad[:6])
+
+
 def run_gpu(z, g, precision, graph=0, bind=False, nsteps=None):
     phys, scheme = int(z["phys"]), int(z["scheme"])
     st = px.Stepper(phys, scheme, precision, list(z["prm"]), float(z["dt"]), g)
@@ -141,17 +148,68 @@ def test_zero_steps_is_identity(cuda):
         assert np.array_equal(a, b)
 
 
-def test_launch_counter_counts_stage_kernels(cuda):
+@pytest.mark.parametrize("fused", [True, False])
+def test_launch_counter_counts_stage_kernels(cuda, fused):
     z, grid, g = load(os.path.join(GOLDEN, "ch2d_rk4.npz"))
     st = px.Stepper(px.PHYS_CH, px.RK4, px.F64, list(z["prm"]), float(z["dt"]), g)
+    st.set_fusion(fused)
+    assert st.launches_per_step == (1 if fused else 4)
     f = [torch.from_numpy(np.ascontiguousarray(z["inputs"][0])).cuda()]
     st.load(f)
+    st.advance(1)  # the first step after a load also fills every ghost layer once
     torch.cuda.synchronize()
     before = px.launch_count()
     st.advance(7)
     torch.cuda.synchronize()
-    assert px.launch_count() - before == 7 * 4
+    assert px.launch_count() - before == 7 * st.launches_per_step
     st.close()
+
+
+FUSED_CASES = [
+    # (phys, n, bc x, bc y, d)
+    (px.PHYS_CH, (70, 37), px.BC_PERIODIC, px.BC_PERIODIC, (1.0, 1.0)),
+    (px.PHYS_CH, (130, 47), px.BC_NOFLUX, px.BC_PERIODIC, (0.9, 1.1)),
+    (px.PHYS_CH, (64, 16), px.BC_PERIODIC, px.BC_NOFLUX, (1.0, 1.0)),
+    (px.PHYS_CH, (9, 30), px.BC_NOFLUX, px.BC_NOFLUX, (1.0, 1.0)),
+    (px.PHYS_AC, (200, 33), px.BC_PERIODIC, px.BC_PERIODIC, (1.0, 0.7)),
+    (px.PHYS_AC, (66, 65), px.BC_NOFLUX, px.BC_NOFLUX, (1.0, 1.0)),
+]
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32])
+@pytest.mark.parametrize("case", range(len(FUSED_CASES)))
+def test_one_launch_step_matches_per_stage_launches(cuda, oracle, prec, case):
+    """The four-stages-in-one-launch RK4 step gives the bits of the per-stage
+    kernels (and, in FP64, of the oracle) on every stored cell but the ghost
+    corners, for periodic and zero-flux sides, odd sizes and partial tiles."""
+    phys, n, bx, by, d = FUSED_CASES[case]
+    bcs = (bx, bx, by, by, 0, 0)
+    g = px.make_grid(n, d, 1, bcs)
+    grid = Grid(n=n, d=d, bc=bcs, bc_val=(0,) * 6)
+    rng = np.random.default_rng(100 + case)
+    lo_hi = (0.3, 0.7) if phys == px.PHYS_CH else (-0.6, 0.6)
+    x = grid.stored_from_phys(rng.uniform(*lo_hi, size=(1, n[1], n[0])))
+    prm = [1.0, 0.6, 1.2, 0.05, 0.95] if phys == px.PHYS_CH else [0.8, 1.3]
+    dt = 0.004 if phys == px.PHYS_CH else 0.02
+    outs = []
+    for fused in (True, False):
+        st = px.Stepper(phys, px.RK4, prec, prm, dt, g)
+        st.set_fusion(fused)
+        assert st.launches_per_step == (1 if fused else 4)
+        t = torch.from_numpy(x.copy()).cuda()
+        st.load([t])
+        st.set_graph(3)
+        st.advance(11)
+        st.store([t])
+        torch.cuda.synchronize()
+        st.close()
+        outs.append(t.cpu().numpy())
+    keep = ~corner_mask(grid)
+    assert np.array_equal(outs[0][keep], outs[1][keep])
+    if prec == px.F64:
+        want = [x.copy()]
+        oracle.advance(want, phys, prm, px.RK4, dt, 11, grid, fma_mode=1)
+        assert np.array_equal(outs[0][keep], want[0][keep])
 
 
 def test_multistep_ch_matches_oracle_and_reference(cuda, oracle):
@@ -171,8 +229,8 @@ def test_multistep_ch_matches_oracle_and_reference(cuda, oracle):
     oracle.advance_ch_multistep(c_o, mu_o, list(z["prm"]), float(z["dt"]), int(z["nsteps"]), grid, fma_mode=1)
     keep = ~corner_mask(grid)
     got_c, got_mu = outs[0].cpu().numpy(), outs[1].cpu().numpy()
-    assert np.array_equal(got_c[keep], c_o[keep])
-    assert np.array_equal(got_mu[keep], mu_o[keep])
+    assert np.array_equal(got_c[keep], c_o[keep]), _where(got_c, c_o, keep)
+    assert np.array_equal(got_mu[keep], mu_o[keep]), _where(got_mu, mu_o, keep)
     assert np.abs(got_c - z["outputs"][0])[keep].max() <= 1e-12
 
 
@@ -199,5 +257,55 @@ def test_multistep_ch_multi_tile_bcs(cuda, oracle, bc):
     st.close()
     oracle.advance_ch_multistep(c, mu, prm, 0.002, 9, grid, fma_mode=1)
     keep = ~corner_mask(grid)
-    assert np.array_equal(got_c[keep], c[keep])
-    assert np.array_equal(got_mu[keep], mu[keep])
+    assert np.array_equal(got_c[keep], c[keep]), _where(got_c, c, keep)
+    assert np.array_equal(got_mu[keep], mu[keep]), _where(got_mu, mu, keep)
+
+
+TILE_CASES = [
+    # (phys, n, bcs, bc values)
+    (px.PHYS_CH, (300, 70), (px.BC_PERIODIC,) * 4, (0,) * 4),
+    (px.PHYS_CH, (131, 45), (px.BC_NOFLUX, px.BC_NOFLUX, px.BC_PERIODIC, px.BC_PERIODIC), (0,) * 4),
+    (px.PHYS_CH, (70, 37), (px.BC_FIXED, px.BC_FIXED, px.BC_NOFLUX, px.BC_NOFLUX), (0.3, 0.6, 0, 0)),
+    (px.PHYS_AC, (129, 33), (px.BC_PERIODIC, px.BC_PERIODIC, px.BC_NONE, px.BC_NONE), (0,) * 4),
+    (px.PHYS_CHAC, (140, 66), (px.BC_NOFLUX, px.BC_NOFLUX, px.BC_PERIODIC, px.BC_PERIODIC), (0,) * 4),
+]
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32])
+@pytest.mark.parametrize("case", range(len(TILE_CASES)))
+def test_stage_tile_shapes_give_identical_bits(cuda, oracle, prec, case):
+    """Every 2-D stage tile shape (column-walking 0..3, generic box -1), with
+    one launch per stage, gives the same bits; FP64 equals the oracle."""
+    phys, n, bc4, bv4 = TILE_CASES[case]
+    bcs, bcv = tuple(bc4) + (0, 0), tuple(bv4) + (0, 0)
+    d = (1.0, 0.9)
+    g = px.make_grid(n, d, 1, bcs, bcv)
+    grid = Grid(n=n, d=d, bc=bcs, bc_val=bcv)
+    rng = np.random.default_rng(200 + case)
+    nf = px.NFIELDS[phys]
+    lo_hi = (-0.6, 0.6) if phys == px.PHYS_AC else (0.3, 0.7)
+    xs = [grid.stored_from_phys(rng.uniform(*lo_hi, size=(1, n[1], n[0]))) for _ in range(nf)]
+    prm = {px.PHYS_CH: [1.0, 0.6, 1.2, 0.05, 0.95], px.PHYS_AC: [0.8, 1.3],
+           px.PHYS_CHAC: [1.0, 0.9, 0.5, 0.7, 1.1]}[phys]
+    dt = 0.02 if phys == px.PHYS_AC else 0.003
+    outs = {}
+    for tile in (-1, 0, 1, 2, 3):
+        st = px.Stepper(phys, px.RK4, prec, prm, dt, g)
+        st.set_fusion(False)
+        st.set_tiles(tile)
+        ts = [torch.from_numpy(x.copy()).cuda() for x in xs]
+        st.load(ts)
+        st.advance(6)
+        st.store(ts)
+        torch.cuda.synchronize()
+        st.close()
+        outs[tile] = [t.cpu().numpy() for t in ts]
+    keep = ~corner_mask(grid)
+    for tile in (0, 1, 2, 3):
+        for a, b in zip(outs[tile], outs[-1]):
+            assert np.array_equal(a[keep], b[keep]), (tile, _where(a, b, keep))
+    if prec == px.F64:
+        want = [x.copy() for x in xs]
+        oracle.advance(want, phys, prm, px.RK4, dt, 6, grid, fma_mode=1)
+        for a, b in zip(outs[0], want):
+            assert np.array_equal(a[keep], b[keep]), _where(a, b, keep)
