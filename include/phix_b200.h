@@ -260,6 +260,23 @@ int phix_reduce_mass_energy(const double* const* fields, int phys, const double*
 /* Same diagnostics on the stepper's own current state (FP32 or FP64). */
 int phix_stepper_diagnostics(phix_stepper_t* h, double* out);
 
+/* Allocation-free variant of phix_reduce_mass_energy, for callers that cannot
+ * allocate device memory (code running while a CUDA graph is being captured,
+ * hosts whose device memory is owned by another runtime or allocator,
+ * real-time loops that forbid allocation).  It calls no cudaMalloc, cudaFree
+ * or allocating library routine: its scratch is one triple per physical row
+ * (n[1]*n[2] rows) in a file-scope device array sized for
+ * PHIX_NOALLOC_MAX_ROWS rows (about 1.5 MiB, held on every GPU that loads the
+ * library until exit); larger grids return PHIX_ERR_ARG.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress), so make
+ * it before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU race and must be serialised.  Synchronous; same outputs
+ * and status codes as phix_reduce_mass_energy.  No counterpart in the
+ * reference (which has no runtime diagnostics). */
+#define PHIX_NOALLOC_MAX_ROWS 65536
+int phix_reduce_mass_energy_noalloc(const double* const* fields, int phys, const double* prm, const phix_grid_t* g,
+                                    double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
         "phix_stepper_current": ([vp], C.c_int),
         "phix_stepper_run_host": ([vp, C.POINTER(vp), C.POINTER(vp), C.c_int], C.c_int),
         "phix_reduce_mass_energy": ([C.POINTER(vp), C.c_int, P, G, P, vp], C.c_int),
+        "phix_reduce_mass_energy_noalloc": ([C.POINTER(vp), C.c_int, P, G, P, vp], C.c_int),
         "phix_batch_create": ([C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_int, G, P, C.c_double], C.c_int),
         "phix_batch_destroy": ([vp], C.c_int),
         "phix_batch_load": ([vp, C.c_int, vp, C.c_int, vp], C.c_int),
@@ -211,6 +212,13 @@ def axpy(dst, src, coeff: float, stream=None):
 def reduce_mass_energy(fields, phys: int, prm: Sequence[float], g: GridT, stream=None):
     out = (C.c_double * 2)()
     check(lib().phix_reduce_mass_energy(_ptrs(fields), phys, _prm(prm), C.byref(g), out, _stream(stream)))
+    return out[0], out[1]
+
+
+def reduce_mass_energy_noalloc(fields, phys: int, prm: Sequence[float], g: GridT, stream=None):
+    """Allocation-free diagnostics (scratch in a static device array)."""
+    out = (C.c_double * 2)()
+    check(lib().phix_reduce_mass_energy_noalloc(_ptrs(fields), phys, _prm(prm), C.byref(g), out, _stream(stream)))
     return out[0], out[1]
 
 
