@@ -8,8 +8,10 @@ M=1, dt=0.005, single-equation RK4 (M*lap(f'(c) - kappa*lap(c), bcs)),
 c0 = 0.5 + U[-0.01, 0.01] (seed 1).
 
 One bench "step" = one output interval: STEPS_PER_INTERVAL RK4 time steps of
-the whole field, replayed from a CUDA graph (one launch per RK4 time step:
-the four stages run in shared memory; --launch stage: one launch per stage).  L2 is flushed (256 MiB write) between timed steps, outside the timed
+the whole field, replayed from a CUDA graph (the library's default launch
+shape: one launch per stage in FP64, one per time step in FP32; --launch
+overrides it).  --workload selects the other configurations (ac2d, chac3d,
+batch), reported with the same keys.  L2 is flushed (256 MiB write) between timed steps, outside the timed
 events.  `value` = cell-updates/s = cells x time steps / device time.
 `e2e` runs the same interval through the C ABI with pinned HOST buffers
 (phix_stepper_run_host: H2D, advance, D2H, synchronise) inside the timed
@@ -114,12 +116,129 @@ def reference_cpu_rate(fields, g, phys, prm, scheme, dt, nsteps):
     return cells * nsteps / el, el
 
 
+# ---------------------------------------------------------------------------
+# workloads: each runner advances its whole field(s) by `K` time steps per
+# bench step and knows its algorithmic bytes and its end-to-end path
+# ---------------------------------------------------------------------------
+WORKLOADS = {
+    "ch2d": ("CH 1024^2 periodic, single-equation RK4, dt=0.005 (spinodal decomposition)",
+             "synthetic: c0 = 0.5 + U[-0.01,0.01], numpy default_rng(1)"),
+    "ac2d": ("AC 128^2 periodic, Euler, dt=0.01, L=kappa=1 (quickstart form)",
+             "synthetic: phi0 = U[-0.05,0.05], numpy default_rng(0)"),
+    "chac3d": ("CH+AC 3-D 256^3, zero-flux x, periodic y/z, coupled RK4, dt=0.002",
+               "synthetic: c0 = 0.4 + U[-0.01,0.01], eta0 = U[0,0.1], numpy default_rng(2)"),
+    "batch": ("64 batched 2-D CH instances, n in {128..1024}, kappa, M per instance, RK4, dt=0.005",
+              "synthetic: per-instance size/kappa/M/mean from numpy default_rng(3)"),
+}
+
+# DRAM bytes (read + write) per time step, from the ncu captures summarised
+# under profiles/; keyed by (workload, dtype, launches per time step).
+TRAFFIC = {}
+
+
+class StepperRun:
+    """One stepper on a single-field or coupled workload (ch2d, ac2d, chac3d)."""
+
+    def __init__(self, px, torch, dev, args):
+        from phix_b200 import workloads
+        if args.workload == "ch2d":
+            g, phys, prm, scheme, dt, _, fields = workloads.ch2d(n=args.n)
+            self.K = STEPS_PER_INTERVAL
+        elif args.workload == "ac2d":
+            g, phys, prm, scheme, dt, _, fields = workloads.ac2d()
+            self.K = 100
+        else:
+            g, phys, prm, scheme, dt, _, fields = workloads.chac3d(n=args.n if args.n != 1024 else 256)
+            self.K = 10
+        self.prec = px.F64 if args.dtype == "f64" else px.F32
+        w = 8 if self.prec == px.F64 else 4
+        self.nf = len(fields)
+        self.cells = g.n[0] * g.n[1] * g.n[2] * self.nf  # field-cell updates per time step
+        # RK4: R u,W k1 | R u,k1 W k2 | R u,k2 W k3 | R u,k1,k2,k3 W u' = 13w; Euler: R u, W u' = 2w
+        self.alg_bytes = (13 if scheme == px.RK4 else 2) * w * self.cells
+        self.fields, self.g, self.phys, self.prm, self.scheme, self.dt = fields, g, phys, prm, scheme, dt
+        self.st = px.Stepper(phys, scheme, self.prec, prm, dt, g)
+        if args.launch != "auto":
+            self.st.set_fusion(args.launch == "step")
+        self.st.set_tiles(args.tiles)
+        self.lps = self.st.launches_per_step
+        self.d = [torch.from_numpy(f).to(dev) for f in fields]
+        self.st.load(self.d)
+        self.st.set_graph(self.K)
+        self.h_in = [torch.from_numpy(f).pin_memory() for f in fields]
+        self.h_out = [torch.empty_like(h).pin_memory() for h in self.h_in]
+        self.io_bytes = sum(f.nbytes for f in fields)
+        self.shape = (f"{g.n[0]}x{g.n[1]}" + (f"x{g.n[2]}" if g.dim == 3 else "")) + f", {self.nf} field(s)"
+
+    def advance(self, stream):
+        self.st.advance(self.K, stream)
+
+    def e2e_step(self):
+        self.st.run_host(self.h_in, self.h_out, self.K)
+
+    def cpu_sample(self, nsteps):
+        return reference_cpu_rate(self.fields, self.g, self.phys, self.prm, self.scheme, self.dt, nsteps)
+
+    def close(self):
+        self.st.close()
+
+
+class BatchRun:
+    """The batched engine on the 64-instance workload."""
+
+    def __init__(self, px, torch, dev, args):
+        from phix_b200 import workloads
+        grids, phys, prms, scheme, dt, _, fields = workloads.ch2d_batch()
+        self.K = 20
+        self.prec = px.F64 if args.dtype == "f64" else px.F32
+        w = 8 if self.prec == px.F64 else 4
+        self.nf = 1
+        self.cells = sum(g.n[0] * g.n[1] for g in grids)
+        self.alg_bytes = 13 * w * self.cells
+        self.b = px.Batch(phys, scheme, self.prec, grids, prms, dt)
+        self.d = [torch.from_numpy(f).to(dev) for f in fields]
+        for i, t in enumerate(self.d):
+            self.b.load(i, t)
+        self.b.autotune(2)
+        self.lps = 4
+        self.b.set_graph(self.K)
+        self.h_in = [torch.from_numpy(f).pin_memory() for f in fields]
+        self.h_out = [torch.empty_like(h).pin_memory() for h in self.h_in]
+        self.io_bytes = sum(f.nbytes for f in fields)
+        self.torch, self.dev = torch, dev
+        self.grids, self.phys, self.prms, self.scheme, self.dt, self.fields = grids, phys, prms, scheme, dt, fields
+        self.shape = f"{len(grids)} instances, {self.cells} cells"
+
+    def advance(self, stream):
+        self.b.advance(self.K, stream)
+
+    def e2e_step(self):
+        for h, d in zip(self.h_in, self.d):
+            d.copy_(h, non_blocking=True)
+        for i, d in enumerate(self.d):
+            self.b.load(i, d)
+        self.b.advance(self.K)
+        for i, d in enumerate(self.d):
+            self.b.store(i, d)
+        for h, d in zip(self.h_out, self.d):
+            h.copy_(d, non_blocking=True)
+        self.torch.cuda.synchronize(self.dev)
+
+    def cpu_sample(self, nsteps):
+        # one 256^2 instance of the batch stands in for the per-instance rate
+        i = next(k for k, g in enumerate(self.grids) if g.n[0] == 256)
+        return reference_cpu_rate([self.fields[i]], self.grids[i], self.phys, self.prms[i], self.scheme, self.dt,
+                                  nsteps)
+
+    def close(self):
+        self.b.close()
+
+
 def bench_ours(args):
     import torch
     import torch.distributed as dist
 
     import phix_b200 as px
-    from phix_b200 import workloads
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -132,24 +251,13 @@ def bench_ours(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    g, phys, prm, scheme, dt, _, fields = workloads.ch2d(n=args.n)
-    cells = g.n[0] * g.n[1] * g.n[2]
-    prec = px.F64 if args.dtype == "f64" else px.F32
-    w = 8 if prec == px.F64 else 4
-    alg_bytes_step = 13 * w * cells  # RK4, one field: R u,W k1 | R u,k1 W k2 | R u,k2 W k3 | R u,k1,k2,k3 W u'
-
-    st = px.Stepper(phys, scheme, prec, prm, dt, g)
-    st.set_fusion(args.launch == "step")
-    st.set_tiles(args.tiles)
-    lps = st.launches_per_step
-    d_in = torch.from_numpy(fields[0]).to(dev)
-    st.load([d_in])
-    st.set_graph(STEPS_PER_INTERVAL)
+    run = (BatchRun if args.workload == "batch" else StepperRun)(px, torch, dev, args)
+    K = run.K
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
     stream = torch.cuda.current_stream(dev)
 
     for _ in range(args.warmup):
-        st.advance(STEPS_PER_INTERVAL, stream)
+        run.advance(stream)
         flush_l2(flush)
     torch.cuda.synchronize(dev)
     if world > 1:
@@ -162,7 +270,7 @@ def bench_ours(args):
         torch.cuda.synchronize(dev)
         for i in range(args.steps):
             starts[i].record(stream)
-            st.advance(STEPS_PER_INTERVAL, stream)
+            run.advance(stream)
             ends[i].record(stream)
             flush_l2(flush)
         torch.cuda.synchronize(dev)
@@ -176,29 +284,36 @@ def bench_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
-    value = world * cells * STEPS_PER_INTERVAL * args.steps / (total_ms / 1e3)
+    value = world * run.cells * K * args.steps / (total_ms / 1e3)
 
-    # roofline: algorithmic bytes of one time step (13w per cell, the traffic
-    # of one launch per stage) over the device time of one time step
-    t_timestep = ms_per_step / 1e3 / STEPS_PER_INTERVAL
-    achieved = alg_bytes_step / t_timestep / 1e9
+    # roofline: algorithmic bytes of one time step (13w per field-cell for RK4,
+    # the traffic of one launch per stage; 2w for Euler) over the device time
+    # of one time step
+    t_timestep = ms_per_step / 1e3 / K
+    achieved = run.alg_bytes / t_timestep / 1e9
     peak, peak_kind = _peaks()
+    w = 8 if run.prec == px.F64 else 4
+    per_cell = run.alg_bytes // (run.cells * w) * w
+    workload, data = WORKLOADS[args.workload]
+    if args.workload == "ch2d" and args.n != 1024:
+        workload = workload.replace("1024^2", f"{args.n}^2")
 
-    # e2e through the C ABI with pinned host buffers
     if args.no_e2e:
-        st.close()
+        run.close()
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
                               "ms_per_step": ms_per_step, "roofline_achieved_gbs": achieved, "n": args.n,
+                              "workload": workload, "dtype": args.dtype, "launches_per_time_step": run.lps,
                               "note": "profiling run (--no-e2e)"}), flush=True)
         if world > 1:
             dist.barrier()
             dist.destroy_process_group()
         return None
-    h_in = torch.from_numpy(fields[0]).pin_memory()
-    h_out = torch.empty_like(h_in).pin_memory()
+
+    # e2e through the public API with pinned host buffers: H2D of the inputs,
+    # K time steps, D2H of the result, every step
     for _ in range(2):
-        st.run_host([h_in], [h_out], STEPS_PER_INTERVAL)
+        run.e2e_step()
     e2e_steps = max(3, args.steps // 2)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -206,7 +321,7 @@ def bench_ours(args):
     e2e_dev2 = torch.cuda.Event(enable_timing=True)
     e2e_dev.record(stream)
     for _ in range(e2e_steps):
-        st.run_host([h_in], [h_out], STEPS_PER_INTERVAL)
+        run.e2e_step()
     e2e_dev2.record(stream)
     torch.cuda.synchronize(dev)
     e2e_wall = time.perf_counter() - t0
@@ -215,20 +330,22 @@ def bench_ours(args):
         t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_value = world * cells * STEPS_PER_INTERVAL * e2e_steps / (e2e_ms / 1e3)
-    stored_bytes = fields[0].nbytes
-    st.close()
+    e2e_value = world * run.cells * K * e2e_steps / (e2e_ms / 1e3)
 
     line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             try:
-                n_cpu = args.cpu_baseline_steps
-                rate, el = reference_cpu_rate(fields, g, phys, prm, scheme, dt, n_cpu)
+                n_cpu = args.cpu_baseline_steps if args.workload != "chac3d" else 1
+                rate, el = run.cpu_sample(n_cpu)
+                if args.workload == "chac3d":
+                    rate *= run.nf  # field-cell updates, like `value`
                 cpu = {"value": rate, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
                        "sample": f"reference CPU path (computeRHSCPU + applyOnCPU, GPU stage semantics), "
-                                 f"{n_cpu} RK4 steps of the same 1024^2 field, {el:.1f} s, 1 thread"}
+                                 f"{n_cpu} time steps of the same workload"
+                                 f"{' (one 256^2 instance)' if args.workload == 'batch' else ''}, "
+                                 f"{el:.1f} s, 1 thread"}
             except Exception as e:  # oracle/_ref not built on this machine
                 cpu = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "reference",
                        "sample": f"unavailable: {e}"}
@@ -244,25 +361,28 @@ def bench_ours(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": args.dtype,
-            "data": DATA,
-            "config": {"workload": WORKLOAD, "cells": cells, "time_steps_per_step": STEPS_PER_INTERVAL,
-                       "launches_per_time_step": lps,
-                       "precision_note": "FP64 stencils" if prec == px.F64 else "FP32 stencils, FP64 reductions",
-                       "l2": "flushed between timed steps (256 MiB write); one step keeps its field L2-resident",
+            "data": data,
+            "config": {"workload": workload, "shape": run.shape, "field_cells": run.cells,
+                       "time_steps_per_step": K, "launches_per_time_step": run.lps,
+                       "precision_note": "FP64 stencils" if run.prec == px.F64
+                       else "FP32 stencils, compensated FP32 state, FP64 reductions",
+                       "l2": "flushed between timed steps (256 MiB write); within a step the fields may stay "
+                             "L2-resident",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "note": f"algorithmic {13 * w} B/cell-update (13w RK4) over the CUDA-event time of "
-                                 f"one time step ({lps} launch{'es' if lps > 1 else ''} per time step); "
-                                 f"peak {peak_kind}"},
+                         "frac": achieved / peak, "traffic": TRAFFIC.get((args.workload, args.dtype, run.lps)),
+                         "note": f"algorithmic {per_cell} B per field-cell update over the CUDA-event time of "
+                                 f"one time step ({run.lps} launch{'es' if run.lps > 1 else ''} per time step); "
+                                 f"peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
             "hbm_gbs_effective": achieved,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": stored_bytes,
-                    "d2h_bytes_per_step": stored_bytes},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": run.io_bytes,
+                    "d2h_bytes_per_step": run.io_bytes},
             "gpu_launches": launches,
             "clocks": clk.result,
         }
         print(json.dumps(line), flush=True)
+    run.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -343,9 +463,11 @@ def main():
     ap.add_argument("--n", type=int, default=1024, help="grid size n x n (the metric is quoted at 1024)")
     ap.add_argument("--cpu-baseline-steps", type=int, default=50)
     ap.add_argument("--ref-sample-steps", type=int, default=2)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ch2d",
+                    help="ch2d: the headline CH 1024^2 case; ac2d, chac3d, batch: the other configurations")
     ap.add_argument("--tiles", type=int, default=-1, help="2-D stage tile shape (phix_stepper_set_tiles)")
-    ap.add_argument("--launch", choices=["step", "stage"], default="step",
-                    help="one launch per RK4 time step (default) or one per stage")
+    ap.add_argument("--launch", choices=["auto", "step", "stage"], default="auto",
+                    help="one launch per RK4 time step, one per stage, or the library default (auto)")
     args = ap.parse_args()
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)  # timing rule: at least 3 untimed warm-up steps

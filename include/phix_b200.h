@@ -156,19 +156,20 @@ int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream);
  * Solver.cu:405-414) between callbacks. */
 int phix_stepper_set_graph(phix_stepper_t* h, int steps_per_graph);
 
-/* 1 (default): where supported, run each RK4 step as one launch that keeps
- * the four stage states in shared memory and recomputes the tile halos;
- * 0: one launch per stage.  Both give the same bits.  No reference
- * counterpart (the reference runs each term and stage as its own kernels). */
+/* 1: where supported, run each RK4 step as one launch that keeps the four
+ * stage states in shared memory and recomputes the tile halos; 0: one launch
+ * per stage.  Both give the same bits.  Default: 1 for FP32 steppers, 0 for
+ * FP64 (the faster of the two on B200 for each).  No reference counterpart
+ * (the reference runs each term and stage as its own kernels). */
 int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step);
 
 /* Kernel launches one time step takes with the current settings. */
 int phix_stepper_launches_per_step(const phix_stepper_t* h);
 
-/* Tile shape of the 2-D per-stage kernels: -1 (default) the box tiles (64x16,
- * 256 threads), 0..3 column-walking tiles (TX x TY = 128x16, 64x16, 64x32,
- * 128x32; one thread per column).  All give the same bits.  No reference
- * counterpart. */
+/* Tile shape of the 2-D per-stage kernels: -1 the box tiles (64x16, 256
+ * threads, flat cell loops), 0..3 column-walking tiles (TX x TY = 64x16,
+ * 64x32, 128x16, 32x16 with 4, 4, 2, 8 row groups; 256 threads).  All give the
+ * same bits.  No reference counterpart. */
 int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg);
 
 /* FP64 only: run directly on caller-owned buffers, no copies.  fields[f] is

@@ -31,21 +31,21 @@ constexpr int BOX_TX = 64, BOX_TY = 16, BOX_NT = 256;
 constexpr int LIN_TX = 256, LIN_NT = 256;
 constexpr int M3_TX = 32, M3_TY = 8, M3_RZ = 16, M3_NT = 256;
 
-// 2-D column-walking tiles (stage_col.cuh): (TX, TY) per configuration.
-constexpr int kColCfgs[][2] = {{128, 16}, {64, 16}, {64, 32}, {128, 32}};
+// 2-D column-walking tiles (stage_col.cuh): (TX, TY, row groups G); TX*G threads.
+constexpr int kColCfgs[][3] = {{64, 16, 4}, {64, 32, 4}, {128, 16, 2}, {32, 16, 8}};
 constexpr int kNumColCfgs = sizeof(kColCfgs) / sizeof(kColCfgs[0]);
 
-template <typename T, class Pol, int MODE, int TX, int TY>
+template <typename T, class Pol, int MODE, int TX, int TY, int G>
 int launch_col_cfg(const StageArgs<T>& A, cudaStream_t s) {
     dim3 grid((A.L.n[0] + TX - 1) / TX, (A.L.n[1] + TY - 1) / TY, 1);
-    stage_col<T, Pol, MODE, TX, TY><<<grid, TX, col_smem_bytes<T, Pol, TX, TY>(), s>>>(A, Pol{});
+    stage_col<T, Pol, MODE, TX, TY, G><<<grid, TX * G, col_smem_bytes<T, Pol, TX, TY>(), s>>>(A, Pol{});
     PHIX_LAUNCH_CHECK("stage_col");
     return PHIX_OK;
 }
 
-template <typename T, class Pol, int MODE, int TX, int TY>
+template <typename T, class Pol, int MODE, int TX, int TY, int G>
 int prepare_col_cfg() {
-    PHIX_TRY_CUDA(cudaFuncSetAttribute(stage_col<T, Pol, MODE, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    PHIX_TRY_CUDA(cudaFuncSetAttribute(stage_col<T, Pol, MODE, TX, TY, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)col_smem_bytes<T, Pol, TX, TY>()));
     return PHIX_OK;
 }
@@ -55,8 +55,8 @@ int col_dispatch(int cfg, bool prepare, const StageArgs<T>* A, cudaStream_t s) {
     switch (cfg) {
 #define PHIX_COL_CASE(i)                                                                         \
     case i:                                                                                      \
-        return prepare ? prepare_col_cfg<T, Pol, MODE, kColCfgs[i][0], kColCfgs[i][1]>()         \
-                       : launch_col_cfg<T, Pol, MODE, kColCfgs[i][0], kColCfgs[i][1]>(*A, s);
+        return prepare ? prepare_col_cfg<T, Pol, MODE, kColCfgs[i][0], kColCfgs[i][1], kColCfgs[i][2]>()  \
+                       : launch_col_cfg<T, Pol, MODE, kColCfgs[i][0], kColCfgs[i][1], kColCfgs[i][2]>(*A, s);
         PHIX_COL_CASE(0)
         PHIX_COL_CASE(1)
         PHIX_COL_CASE(2)
@@ -331,7 +331,7 @@ struct phix_stepper {
     // of padding planes; the fused kernels keep the physical plane's ghosts
     // current from then on.
     bool bc_pending = false;
-    bool fuse_steps = true;  // one launch per RK4 step where step2d supports the grid
+    bool fuse_steps = true;  // one launch per RK4 step where step2d supports the grid (FP32 default)
     int tile = -1;           // 2-D stage tiles: -1 generic box tiles (fastest measured), else kColCfgs index
     cudaStream_t cap = nullptr;
     int graph_steps = 0;
@@ -492,6 +492,9 @@ int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precisio
     h->L = L;
     h->S = S;
     h->esz = precision == PHIX_F32 ? 4 : 8;
+    // measured on B200 at 1024^2: the one-launch step wins in FP32 and loses in
+    // FP64 (twice the shared memory per tile, half the resident tiles)
+    h->fuse_steps = precision == PHIX_F32;
     auto fail = [&](cudaError_t e, const char* w) {
         int r = cuda_status(e, w);
         phix_stepper_destroy(h);
