@@ -18,6 +18,7 @@ and on a violation the FD solver takes over for the next `recheck` steps.
 """
 from __future__ import annotations
 
+import os
 import time
 from dataclasses import dataclass, field
 
@@ -31,6 +32,7 @@ KAPPA, MOB, DT = 0.5, 1.0, 0.005
 PRM = [MOB, KAPPA, 1.0, 0.0, 1.0]
 STEPS_PER_CALL = 50
 IN_SHIFT, IN_SCALE, OUT_SCALE = 0.5, 4.0, 0.01
+PARAMS_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "surrogate_ch512.npz")
 
 
 def initial_field(seed: int, n: int = N) -> np.ndarray:
@@ -51,55 +53,82 @@ class TrainLog:
     seconds_fd: float = 0.0
     seconds_train: float = 0.0
     pairs: int = 0
+    updates: int = 0
+
+
+def generate(seeds, nsteps: int, every: int = STEPS_PER_CALL, n: int = N, precision=F32):
+    """FD trajectories of `seeds` on the batched engine: a [len(seeds),
+    nsteps // every + 1, n, n] float64 CUDA tensor of snapshots every `every`
+    time steps (snapshot 0 = the initial field)."""
+    import torch
+    g = make_grid((n, n))
+    ns = nsteps // every + 1
+    data = torch.empty((len(seeds), ns, n, n), dtype=torch.float64, device="cuda")
+    b = Batch(PHYS_CH, RK4, precision, [g] * len(seeds), [PRM] * len(seeds), DT)
+    stored = torch.zeros((len(seeds),) + tuple(stored_shape(g)), dtype=torch.float64, device="cuda")
+    for i, sd in enumerate(seeds):
+        stored[i].copy_(torch.from_numpy(_stored(g, initial_field(sd, n))))
+        b.load(i, stored[i])
+    b.set_graph(every)
+
+    def snapshot(k):
+        for i in range(len(seeds)):
+            b.store(i, stored[i])
+            plane_gather(stored[i], data[i, k], n, n, 1)
+
+    snapshot(0)
+    for k in range(1, ns):
+        b.advance(every)
+        snapshot(k)
+    torch.cuda.synchronize()
+    b.close()
+    return data
 
 
 def train(seeds, nsteps: int = 40000, every: int = STEPS_PER_CALL, batch: int = 16, lr: float = 1e-3,
-          updates_per_snapshot: int = 1, init_seed: int = 0, n: int = N, params=None, log_every: int = 0):
-    """Train on FD trajectories generated on the fly; returns (flat params, log)."""
+          chunk: int = 25, epochs: int = 1, lr_final: float = 1e-4, init_seed: int = 0, n: int = N, params=None,
+          log_every: int = 0, shuffle_seed: int = 0):
+    """Train on FD trajectories generated chunk by chunk (`chunk` trajectories
+    at a time, kept on the GPU): `epochs` passes over the chunk's shuffled
+    (c_t, c_{t+every}) pairs per chunk, Adam with a learning rate decaying
+    geometrically from `lr` to `lr_final` over the whole run.  Returns (flat
+    params, log)."""
     import torch
-
     if params is None:
         params = init_params(init_seed)
     sg = Surrogate(n, n, batch, IN_SHIFT, IN_SCALE, OUT_SCALE)
     sg.set_params(params)
     log = TrainLog()
-    g = make_grid((n, n))
     seeds = list(seeds)
-    for start in range(0, len(seeds), batch):
-        chunk = seeds[start:start + batch]
-        b = Batch(PHYS_CH, RK4, F32, [g] * len(chunk), [PRM] * len(chunk), DT)
-        for i, s in enumerate(chunk):
-            b.load(i, _stored(g, initial_field(s, n)))
-        b.set_graph(every)
-        stored = torch.zeros((len(chunk),) + tuple(stored_shape(g)), dtype=torch.float64, device="cuda")
-        prev = torch.empty((len(chunk), n, n), dtype=torch.float64, device="cuda")
-        cur = torch.empty_like(prev)
-
-        def snapshot(dst):
-            for i in range(len(chunk)):
-                b.store(i, stored[i])
-                plane_gather(stored[i], dst[i], n, n, 1)
-
-        snapshot(prev)
-        for k in range(nsteps // every):
-            t0 = time.perf_counter()
-            b.advance(every)
-            snapshot(cur)
-            torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            for _ in range(updates_per_snapshot):
-                loss = sg.grad(prev, cur)
-                sg.adam(lr)
-            torch.cuda.synchronize()
-            t2 = time.perf_counter()
-            log.seconds_fd += t1 - t0
-            log.seconds_train += t2 - t1
-            log.losses.append(loss)
-            log.pairs += len(chunk)
-            if log_every and k % log_every == 0:
-                print(f"chunk {start // batch} snap {k}: loss {loss:.4e}", flush=True)
-            prev, cur = cur, prev
-        b.close()
+    rng = np.random.default_rng(shuffle_seed)
+    ns = nsteps // every + 1
+    total = max(1, (len(seeds) * (ns - 1) * epochs) // batch)
+    for start in range(0, len(seeds), chunk):
+        t0 = time.perf_counter()
+        data = generate(seeds[start:start + chunk], nsteps, every, n)
+        log.seconds_fd += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        T = data.shape[0]
+        npairs = T * (ns - 1)
+        for _ in range(epochs):
+            perm = torch.from_numpy(rng.permutation(npairs)).cuda()
+            for j in range(0, npairs - batch + 1, batch):
+                idx = perm[j:j + batch]
+                ti, si = idx // (ns - 1), idx % (ns - 1)
+                a = data[ti, si].contiguous()
+                nxt = data[ti, si + 1].contiguous()
+                loss = sg.grad(a, nxt)
+                rate = lr * (lr_final / lr) ** min(1.0, log.updates / total)
+                sg.adam(rate)
+                log.updates += 1
+                log.pairs += batch
+                log.losses.append(loss)
+                if log_every and log.updates % log_every == 0:
+                    print(f"update {log.updates}/{total}: loss {np.mean(log.losses[-log_every:]):.4e} "
+                          f"lr {rate:.2e}", flush=True)
+        torch.cuda.synchronize()
+        log.seconds_train += time.perf_counter() - t0
+        del data
     p, _ = sg.get_params()
     sg.close()
     return p, log
@@ -229,3 +258,148 @@ def _recheck_ok(g, c_old, c_new, stored, rhs, resid_tol):
         return False
     rate = (c_new - c_old) / (STEPS_PER_CALL * DT)
     return _rhs_norms(g, c_old, stored, rhs, rate) <= resid_tol
+
+
+# ---------------------------------------------------------------------------
+# evaluation and timing
+# ---------------------------------------------------------------------------
+def _rel(a, b):
+    import torch
+    return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+
+
+def _rel_fluct(a, b):
+    import torch
+    return float(torch.linalg.norm(a - b) / torch.linalg.norm(b - b.mean()))
+
+
+def evaluate(params: np.ndarray, seeds, checkpoints=(1, 10, 50, 100, 200, 400, 800), n: int = N):
+    """Pure surrogate rollouts (no FD take-over) of held-out seeds against the
+    FP64 fused FD solution at the same times.  Per seed and checkpoint (in
+    surrogate steps of STEPS_PER_CALL FD steps): rel-L2 = ||c_s - c_fd|| /
+    ||c_fd||, the same relative to the fluctuation ||c_fd - mean||, the
+    no-network baseline (c stays c0) on both measures, and the mass drift."""
+    import torch
+    g = make_grid((n, n))
+    sg = Surrogate(n, n, 1, IN_SHIFT, IN_SCALE, OUT_SCALE)
+    sg.set_params(params)
+    rows = []
+    for sd in seeds:
+        c0 = initial_field(sd, n)
+        # FD FP64 at the checkpoints
+        st = Stepper(PHYS_CH, RK4, F64, PRM, DT, g)
+        d = torch.from_numpy(_stored(g, c0)).cuda()
+        st.load([d])
+        st.set_graph(STEPS_PER_CALL)
+        fd = {}
+        done = 0
+        plane = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        for cp in checkpoints:
+            st.advance((cp - done) * STEPS_PER_CALL)
+            done = cp
+            st.store([d])
+            plane_gather(d, plane, n, n, 1)
+            fd[cp] = plane.clone()
+        st.close()
+        # surrogate
+        a = torch.from_numpy(c0.copy()).cuda()[None]
+        b = torch.empty_like(a)
+        c0t = a[0].clone()
+        k = 0
+        for cp in checkpoints:
+            while k < cp:
+                sg.step(a, b)
+                a, b = b, a
+                k += 1
+            ref = fd[cp]
+            rows.append({"seed": sd, "step": cp, "rel_l2": _rel(a[0], ref), "rel_l2_fluct": _rel_fluct(a[0], ref),
+                         "baseline_rel_l2": _rel(c0t, ref), "baseline_rel_l2_fluct": _rel_fluct(c0t, ref),
+                         "mass_rel": abs(float(a[0].mean() - c0t.mean())) / abs(float(c0t.mean()))})
+    sg.close()
+    return rows
+
+
+def time_speed(params: np.ndarray, sur_steps: int = 40, n: int = N, warmup: int = 3):
+    """Device time of `sur_steps` surrogate steps (batch 1, with the mass
+    projection) against the fused FD solver advancing the same simulated time
+    (sur_steps * STEPS_PER_CALL steps) in FP32 and FP64; CUDA events on the
+    launching stream, graphs for the FD steps.  Returns a dict of ms."""
+    import torch
+    g = make_grid((n, n))
+    c0 = initial_field(100, n)
+    sg = Surrogate(n, n, 1, IN_SHIFT, IN_SCALE, OUT_SCALE)
+    sg.set_params(params)
+    a = torch.from_numpy(c0.copy()).cuda()[None]
+    b = torch.empty_like(a)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(warmup):
+        sg.step(a, b)
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(sur_steps):
+        sg.step(a, b)
+        a, b = b, a
+    ev[1].record()
+    torch.cuda.synchronize()
+    out = {"surrogate_ms": ev[0].elapsed_time(ev[1])}
+    sg.close()
+    for prec, key in ((F32, "fd_f32_ms"), (F64, "fd_f64_ms")):
+        st = Stepper(PHYS_CH, RK4, prec, PRM, DT, g)
+        d = torch.from_numpy(_stored(g, c0)).cuda()
+        st.load([d])
+        st.set_graph(STEPS_PER_CALL)
+        for _ in range(warmup):
+            st.advance(STEPS_PER_CALL)
+        torch.cuda.synchronize()
+        ev[0].record()
+        st.advance(sur_steps * STEPS_PER_CALL)
+        ev[1].record()
+        torch.cuda.synchronize()
+        out[key] = ev[0].elapsed_time(ev[1])
+        st.close()
+    out["sim_time"] = sur_steps * STEPS_PER_CALL * DT
+    return out
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train / evaluate / time the CH 512^2 surrogate")
+    ap.add_argument("cmd", choices=["train", "evaluate", "time"])
+    ap.add_argument("--params", default=PARAMS_FILE)
+    ap.add_argument("--seeds", default="100:300", help="training seeds lo:hi")
+    ap.add_argument("--eval-seeds", default="300:304")
+    ap.add_argument("--nsteps", type=int, default=40000)
+    ap.add_argument("--epochs", type=int, default=1)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr-final", type=float, default=1e-4)
+    ap.add_argument("--chunk", type=int, default=25)
+    ap.add_argument("--log-every", type=int, default=500)
+    args = ap.parse_args(argv)
+    lo, hi = (int(v) for v in args.seeds.split(":"))
+    elo, ehi = (int(v) for v in args.eval_seeds.split(":"))
+    if args.cmd == "train":
+        p, log = train(range(lo, hi), nsteps=args.nsteps, batch=args.batch, lr=args.lr, lr_final=args.lr_final,
+                       chunk=args.chunk, epochs=args.epochs, log_every=args.log_every)
+        np.savez(args.params, params=p, seeds=np.arange(lo, hi), nsteps=args.nsteps, epochs=args.epochs,
+                 losses=np.asarray(log.losses[::10], np.float32))
+        print(json.dumps({"updates": log.updates, "pairs": log.pairs, "seconds_fd": log.seconds_fd,
+                          "seconds_train": log.seconds_train, "loss_first": float(np.mean(log.losses[:50])),
+                          "loss_last": float(np.mean(log.losses[-50:]))}))
+    else:
+        p = load_params(args.params)
+        if args.cmd == "evaluate":
+            for r in evaluate(p, range(elo, ehi)):
+                print(json.dumps(r))
+        else:
+            print(json.dumps(time_speed(p)))
+
+
+def load_params(path: str = PARAMS_FILE) -> np.ndarray:
+    """Trained parameters (flat FP32 vector) saved by `python -m phix_b200.surrogate train`."""
+    return np.load(path)["params"].astype(np.float32)
+
+
+if __name__ == "__main__":
+    main()
