@@ -186,6 +186,172 @@ __global__ void __launch_bounds__(NT) conv32_tc(const ConvArgs a) {
     if (warp == 0) tc::tmem_dealloc(tmem, 32);
 }
 
+// ---------------------------------------------------------------------------
+// Forward 32 -> 32 convolution, row-pipelined.  A CTA owns strips of
+// `rows` consecutive output rows of one 128-pixel column segment and walks
+// them top to bottom with a ring of 6 staged input rows: each output row
+// stages one new input row (cp.async, issued two rows ahead), the 18 UMMAs of
+// row y run into TMEM accumulator y&1 while the epilogue (bias, GELU, BF16
+// store) of row y-1 drains the other accumulator.  Same arithmetic as
+// conv32_tc<EPI_FWD> except GELU's tanh, which uses the hardware tanh.approx
+// instruction.
+// ---------------------------------------------------------------------------
+constexpr int RING = 6;
+constexpr int NT_ROWS = 256;  // 8 warps: warp w drains TMEM lanes 32*(w%4).. and channels 16*(w/4)..
+
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float gelu_hw(float x) {
+    const float k = 0.7978845608028654f, c = 0.044715f;
+    return 0.5f * x * (1.0f + tanh_hw(k * (x + c * x * x * x)));
+}
+
+// Stage input row gy (wrapped) of image b, pixels x0-1 .. x0+TILE, into ring slot `slot`
+// (cp.async by the NTH threads of the CTA).
+template <int NTH = NT_ROWS>
+__device__ __forceinline__ void stage_row_async(uint32_t rows_a, int slot, const __nv_bfloat16* __restrict__ x, int b,
+                                                int gy, int x0, int H, int W) {
+    gy = wrap(gy, H);
+    const __nv_bfloat16* src = x + ((size_t)b * H + gy) * W * CH;
+#pragma unroll
+    for (int u = threadIdx.x; u < HALO_PX * 4; u += NTH) {
+        const int i = u >> 2, j = u & 3;
+        const int gx = wrap(x0 - 1 + i, W);
+        cp_async16(rows_a + slot * ROW_B + j * CHUNK_B + i * 16, src + (size_t)gx * CH + j * 8);
+    }
+}
+
+__global__ void __launch_bounds__(NT_ROWS) conv32_rows_tc(const ConvArgs a, int rows) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    uint8_t* wbuf = sm;
+    uint8_t* ring = sm + WPK_B;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + WPK_B + RING * ROW_B);  // 2 barriers
+    uint32_t* slot_t = reinterpret_cast<uint32_t*>(bar + 2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    for (int u = threadIdx.x; u < WPK_B / 16; u += NT_ROWS)
+        reinterpret_cast<uint4*>(wbuf)[u] = __ldg(reinterpret_cast<const uint4*>(a.wpk) + u);
+    if (warp == 0) {
+        tc::tmem_alloc(slot_t, 64);
+        tc::tmem_relinquish();
+    }
+    if (threadIdx.x == 0) {
+        tc::mbar_init(bar, 1);
+        tc::mbar_init(bar + 1, 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot_t;
+    const uint32_t idesc = tc::idesc_bf16_f32(128, 32, 0, 0);
+    const uint32_t ring_a = tc::smem_u32(ring), w_a = tc::smem_u32(wbuf);
+    const int quad = warp & 3, half = warp >> 2;  // TMEM lane quadrant, channel half
+    float bias[16];
+#pragma unroll
+    for (int n = 0; n < 16; ++n) bias[n] = __ldg(a.bias + 16 * half + n);
+
+    const int tpr = a.W / TILE;
+    const int nstrips = (a.H + rows - 1) / rows;
+    const int njobs = a.B * tpr * nstrips;
+    uint32_t phase[2] = {0u, 0u};
+    bool failed = false;
+    for (int job = blockIdx.x; job < njobs && !failed; job += gridDim.x) {
+        const int b = job / (tpr * nstrips), rem = job - b * tpr * nstrips;
+        const int strip = rem / tpr, x0 = (rem - strip * tpr) * TILE;
+        const int y0 = strip * rows, y1 = min(y0 + rows, a.H);
+        // rows y0-1, y0, y0+1 -> slots 0, 1, 2 (slot of row r: (r - y0 + 1) % RING),
+        // then y0+2 as its own group (two rows in flight ahead of the UMMAs)
+        for (int r = 0; r < 3; ++r) stage_row_async(ring_a, r, a.x, b, y0 - 1 + r, x0, a.H, a.W);
+        cp_async_commit();
+        if (y0 + 2 <= y1) stage_row_async(ring_a, 3, a.x, b, y0 + 2, x0, a.H, a.W);
+        cp_async_commit();
+        auto epilogue = [&](int y) {
+            const int acc = y & 1;
+            if (!tc::mbar_wait_bounded(bar + acc, phase[acc], WAIT_NS)) {
+                failed = true;
+                return;
+            }
+            phase[acc] ^= 1u;
+            tc::fence_after_sync();
+            float v[16];
+            tc::tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(acc * 32 + 16 * half), v);
+            const int gx = x0 + quad * 32 + lane;
+            const size_t o = (((size_t)b * a.H + y) * a.W + gx) * CH + 16 * half;
+#pragma unroll
+            for (int n = 0; n < 16; ++n) v[n] += bias[n];
+            if (a.zout) {
+                uint4* zd = reinterpret_cast<uint4*>(a.zout + o);
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                    zd[q] = make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
+                                       pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
+            }
+#pragma unroll
+            for (int n = 0; n < 16; ++n) v[n] = gelu_hw(v[n]);
+            uint4* dst = reinterpret_cast<uint4*>(a.out + o);
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+                dst[q] = make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
+                                    pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
+        };
+        for (int y = y0; y < y1; ++y) {
+            // rows y-1 .. y+1 resident (this thread's copies, then everyone's;
+            // the newest group, row y+2, may still be in flight); a timed-out
+            // wait anywhere in the CTA stops every thread here
+            cp_async_wait_one();
+            tc::fence_async_smem();
+            tc::fence_before_sync();
+            if (__syncthreads_or(failed)) {
+                failed = true;
+                break;
+            }
+            tc::fence_after_sync();
+            if (threadIdx.x == 0) {
+                const int acc = y & 1;
+#pragma unroll
+                for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk) {
+                        const int ky = tap / 3, kx = tap % 3;
+                        const int slot = (y - 1 + ky - y0 + 1) % RING;
+                        const uint64_t ad =
+                            tc::sdesc(ring_a + slot * ROW_B + 2 * kk * CHUNK_B + kx * 16, CHUNK_B, 128);
+                        const uint64_t bd = tc::sdesc(w_a + (tap * 2 + kk) * 1024, 512, 128);
+                        tc::umma_bf16(tmem + (uint32_t)(acc * 32), ad, bd, idesc, (tap | kk) != 0);
+                    }
+                tc::umma_commit(bar + acc);
+            }
+            // input row y+3 into the slot of row y-3 (its last reader, row y-2's
+            // UMMAs, completed before row y-2's epilogue ran in the previous
+            // iteration); an empty group keeps the group count uniform
+            if (y + 3 <= y1) stage_row_async(ring_a, (y + 3 - y0 + 1) % RING, a.x, b, y + 3, x0, a.H, a.W);
+            cp_async_commit();
+            if (y > y0) epilogue(y - 1);
+        }
+        if (!failed) epilogue(y1 - 1);
+        // the ring is reused by the next strip
+        cp_async_wait_all();
+        tc::fence_before_sync();
+        failed = __syncthreads_or(failed);
+        tc::fence_after_sync();
+    }
+    if (failed && threadIdx.x == 0) atomicExch(a.err, 1);
+    cp_async_wait_all();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 64);
+}
+
 struct WgradArgs {
     const __nv_bfloat16* x;   // layer input [B][H][W][32]
     const __nv_bfloat16* dz;  // gradient w.r.t. the layer's pre-activation
@@ -318,9 +484,9 @@ __global__ void __launch_bounds__(256) layer1_fwd(const double* __restrict__ c, 
                 for (int t = 0; t < 9; ++t) s = fmaf(xv[t], ws[n * 9 + t], s);
                 z[e] = s + bs[n];
             }
-            zd[q] = make_uint4(pack2(z[0], z[1]), pack2(z[2], z[3]), pack2(z[4], z[5]), pack2(z[6], z[7]));
-            hd[q] = make_uint4(pack2(gelu_f(z[0]), gelu_f(z[1])), pack2(gelu_f(z[2]), gelu_f(z[3])),
-                               pack2(gelu_f(z[4]), gelu_f(z[5])), pack2(gelu_f(z[6]), gelu_f(z[7])));
+            if (z1) zd[q] = make_uint4(pack2(z[0], z[1]), pack2(z[2], z[3]), pack2(z[4], z[5]), pack2(z[6], z[7]));
+            hd[q] = make_uint4(pack2(gelu_hw(z[0]), gelu_hw(z[1])), pack2(gelu_hw(z[2]), gelu_hw(z[3])),
+                               pack2(gelu_hw(z[4]), gelu_hw(z[5])), pack2(gelu_hw(z[6]), gelu_hw(z[7])));
         }
     }
 }
@@ -356,6 +522,125 @@ __global__ void __launch_bounds__(256) layer4_fwd(const __nv_bfloat16* __restric
         if (o_out) o_out[p] = o;
         if (c_out) c_out[p] = c[p] + P.out_scale * (double)o;
     }
+}
+
+// Layer 4 on 128-pixel row segments staged in shared memory (3 input rows,
+// [row][chunk][pixel][8 channels], circular wrap).  Block (bx, image) takes a
+// contiguous range of the image's segments ordered segment-major, so
+// consecutive segments are consecutive rows and each one stages a single new
+// row.  Also writes c_out = c + out_scale * o and this block's FP64 sums of c
+// and c_out to part[(image * gridDim.x + bx) * 2 + {0, 1}] for the mass
+// projection (fixed order, so the result is deterministic).
+constexpr int L4_MAXBLK = 2048;
+
+__global__ void __launch_bounds__(NT) layer4_rows(const __nv_bfloat16* __restrict__ h3, const float* __restrict__ w4,
+                                                  const float* __restrict__ b4, const double* __restrict__ c,
+                                                  double* __restrict__ c_out, float* __restrict__ o_out, int H, int W,
+                                                  NetParams P, double* __restrict__ part) {
+    __shared__ __align__(16) uint8_t rows[3 * ROW_B];
+    __shared__ float ws[9 * 32];
+    __shared__ double red[2][NT / 32];
+    const uint32_t rows_a = tc::smem_u32(rows);
+    for (int i = threadIdx.x; i < 9 * 32; i += NT) ws[i] = w4[i];
+    const int b = blockIdx.y;
+    const int tpr = W / TILE, ntile = H * tpr;
+    const int per = (ntile + gridDim.x - 1) / gridDim.x;
+    const int t0 = blockIdx.x * per, t1 = min(t0 + per, ntile);
+    const float bias = b4[0];
+    double sc = 0.0, so = 0.0;
+    int have = -1000000, seg_have = -1;  // row resident in slot (row % 3) up to `have`
+    for (int t = t0; t < t1; ++t) {
+        const int seg = t / H, y = t - seg * H, x0 = seg * TILE;
+        __syncthreads();  // previous tile done with the rows about to be replaced
+        const bool cont = seg == seg_have && y == have;  // rows y-2 .. y resident: stage only y+1
+        for (int r = cont ? 2 : 0; r < 3; ++r)
+            stage_row_async<NT>(rows_a, ((y - 1 + r) % 3 + 3) % 3, h3, b, y - 1 + r, x0, H, W);
+        cp_async_commit();
+        cp_async_wait_all();
+        have = y + 1;
+        seg_have = seg;
+        __syncthreads();
+        float s = 0.f;
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+            const int slot = ((y - 1 + ky) % 3 + 3) % 3;
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    float f[8];
+                    unpack8(*reinterpret_cast<const uint4*>(rows + slot * ROW_B + k * CHUNK_B + (threadIdx.x + kx) * 16),
+                            f);
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) s = fmaf(f[e], ws[(ky * 3 + kx) * 32 + 8 * k + e], s);
+                }
+            }
+        }
+        const size_t p = ((size_t)b * H + y) * W + x0 + threadIdx.x;
+        const float o = s + bias;
+        if (o_out) o_out[p] = o;
+        if (c_out) {
+            const double cv = c[p], co = cv + P.out_scale * (double)o;
+            c_out[p] = co;
+            sc += cv;
+            so += co;
+        }
+    }
+    if (!c_out) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sc += __shfl_xor_sync(0xffffffffu, sc, o);
+        so += __shfl_xor_sync(0xffffffffu, so, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = sc; red[1][threadIdx.x >> 5] = so; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0.0, a1 = 0.0;
+        for (int w = 0; w < NT / 32; ++w) { a0 += red[0][w]; a1 += red[1][w]; }
+        part[((size_t)b * gridDim.x + blockIdx.x) * 2 + 0] = a0;
+        part[((size_t)b * gridDim.x + blockIdx.x) * 2 + 1] = a1;
+    }
+}
+
+// Mass correction per image from layer4_rows' partials: one warp per image,
+// lane l sums partials l, l+32, ... (8 independent accumulators, then a fixed
+// combination and a fixed shuffle tree, so the result is deterministic).
+__global__ void __launch_bounds__(32) mass_correction(const double* __restrict__ part, int nparts, size_t npix,
+                                                      double* __restrict__ corr) {
+    const int img = blockIdx.x;
+    double sa[8] = {0, 0, 0, 0, 0, 0, 0, 0}, sb[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const double* pp = part + (size_t)img * nparts * 2;
+    for (int k0 = threadIdx.x; k0 < nparts; k0 += 32 * 8) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int k = k0 + 32 * q;
+            if (k < nparts) {
+                sa[q] += pp[2 * k];
+                sb[q] += pp[2 * k + 1];
+            }
+        }
+    }
+    double a = 0.0, b = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        a += sa[q];
+        b += sb[q];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (threadIdx.x == 0) corr[img] = (a - b) / (double)npix;
+}
+
+// c_out += corr[image]: the mean-mass projection.
+__global__ void __launch_bounds__(256) apply_correction(double* __restrict__ c_out, const double* __restrict__ corr,
+                                                        size_t npix) {
+    const int img = blockIdx.y;
+    const double cr = corr[img];
+    for (size_t p = blockIdx.x * 256ull + threadIdx.x; p < npix; p += (size_t)gridDim.x * 256)
+        c_out[img * npix + p] += cr;
 }
 
 // Per-image FP64 sums of a and b (grid-stride per image: one block row per image).
@@ -632,32 +917,52 @@ int sg_pack(phix_surrogate* s, cudaStream_t st) {
     return PHIX_OK;
 }
 
-int sg_forward(phix_surrogate* s, const double* c, int B, double* c_out, float* o_out, cudaStream_t st) {
+constexpr size_t ROWS_SMEM = WPK_B + RING * ROW_B + 2 * 8 + 8;
+
+int sg_conv_rows(phix_surrogate* s, const ConvArgs& a, cudaStream_t st) {
+    const int tpr = a.W / TILE;
+    const long long tiles = (long long)a.B * a.H * tpr;
+    const int slots = s->nsm * 3;  // 3 CTAs of ~60 KB shared memory per SM
+    int rows = (int)((tiles + slots - 1) / slots);
+    if (rows < 2) rows = 2;
+    const long long jobs = (long long)a.B * tpr * ((a.H + rows - 1) / rows);
+    const int grid = (int)(jobs < slots ? jobs : slots);
+    conv32_rows_tc<<<grid, NT_ROWS, ROWS_SMEM, st>>>(a, rows);
+    PHIX_LAUNCH_CHECK("conv32_rows_tc");
+    return PHIX_OK;
+}
+
+int sg_forward(phix_surrogate* s, const double* c, int B, double* c_out, float* o_out, cudaStream_t st,
+               bool keep_z = true) {
     int rc;
     if (!s->packed && (rc = sg_pack(s, st))) return rc;
     const size_t N = (size_t)B * s->H * s->W;
     const int eg = (int)((N + 255) / 256 < (size_t)s->nsm * 8 ? (N + 255) / 256 : (size_t)s->nsm * 8);
-    layer1_fwd<<<eg, 256, 0, st>>>(c, s->w1r, s->params + OFF_B1, s->z1, s->h1, B, s->H, s->W, s->P);
+    layer1_fwd<<<eg, 256, 0, st>>>(c, s->w1r, s->params + OFF_B1, keep_z ? s->z1 : nullptr, s->h1, B, s->H, s->W,
+                                   s->P);
     PHIX_LAUNCH_CHECK("layer1_fwd");
-    const size_t smem = WPK_B + 3 * ROW_B + 16;
-    const int cg = sg_conv_grid(s, B);
     ConvArgs a{};
     a.B = B; a.H = s->H; a.W = s->W; a.err = s->err;
-    a.x = s->h1; a.wpk = s->pk; a.bias = s->params + OFF_B2; a.out = s->h2; a.zout = s->z2;
-    conv32_tc<EPI_FWD><<<cg, NT, smem, st>>>(a);
-    PHIX_LAUNCH_CHECK("conv32_tc<fwd>");
-    a.x = s->h2; a.wpk = s->pk + 9216; a.bias = s->params + OFF_B3; a.out = s->h3; a.zout = s->z3;
-    conv32_tc<EPI_FWD><<<cg, NT, smem, st>>>(a);
-    PHIX_LAUNCH_CHECK("conv32_tc<fwd>");
-    layer4_fwd<<<eg, 256, 0, st>>>(s->h3, s->w4r, s->params + OFF_B4, c, c_out, o_out, B, s->H, s->W, s->P);
-    PHIX_LAUNCH_CHECK("layer4_fwd");
+    a.x = s->h1; a.wpk = s->pk; a.bias = s->params + OFF_B2; a.out = s->h2; a.zout = keep_z ? s->z2 : nullptr;
+    if ((rc = sg_conv_rows(s, a, st))) return rc;
+    a.x = s->h2; a.wpk = s->pk + 9216; a.bias = s->params + OFF_B3; a.out = s->h3; a.zout = keep_z ? s->z3 : nullptr;
+    if ((rc = sg_conv_rows(s, a, st))) return rc;
+    const int tiles = s->H * (s->W / TILE);
+    int nb = (tiles + 1) / 2;  // two segments (consecutive rows) per block
+    nb = nb < L4_MAXBLK ? nb : L4_MAXBLK;
+    layer4_rows<<<dim3(nb, B), NT, 0, st>>>(s->h3, s->w4r, s->params + OFF_B4, c, c_out, o_out, s->H, s->W, s->P,
+                                            s->sums);
+    PHIX_LAUNCH_CHECK("layer4_rows");
     if (c_out) {
         const size_t npix = (size_t)s->H * s->W;
-        dim3 g(64, B);
-        image_sums<<<g, 256, 0, st>>>(c, c_out, npix, s->sums);
-        PHIX_LAUNCH_CHECK("image_sums");
-        project_mass<<<g, 256, 0, st>>>(c_out, s->sums, 64, npix);
-        PHIX_LAUNCH_CHECK("project_mass");
+        int pb = (int)((npix + 255) / 256);
+        const int pmax = (s->nsm * 4 + B - 1) / B;
+        pb = pb < pmax ? pb : pmax;
+        double* corr = s->sums + (size_t)2 * L4_MAXBLK * s->bmax;
+        mass_correction<<<B, 32, 0, st>>>(s->sums, nb, npix, corr);
+        PHIX_LAUNCH_CHECK("mass_correction");
+        apply_correction<<<dim3(pb, B), 256, 0, st>>>(c_out, corr, npix);
+        PHIX_LAUNCH_CHECK("apply_correction");
     }
     return PHIX_OK;
 }
@@ -679,6 +984,8 @@ int phix_surrogate_create(phix_surrogate_t** out, int H, int W, int batch_max, d
     {
         cudaError_t ea = cudaFuncSetAttribute(conv32_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, WGRAD_SMEM);
         if (ea != cudaSuccess) { delete s; return cuda_status(ea, "cudaFuncSetAttribute(wgrad)"); }
+        ea = cudaFuncSetAttribute(conv32_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROWS_SMEM);
+        if (ea != cudaSuccess) { delete s; return cuda_status(ea, "cudaFuncSetAttribute(conv rows)"); }
     }
     s->P.in_shift = in_shift; s->P.in_scale = in_scale; s->P.out_scale = out_scale;
     int dev = 0;
@@ -693,7 +1000,7 @@ int phix_surrogate_create(phix_surrogate_t** out, int H, int W, int batch_max, d
     A((void**)&s->pk, 4 * 9216 * 2); A((void**)&s->w1r, 288 * 4); A((void**)&s->w4r, 288 * 4);
     for (auto** p : {&s->z1, &s->h1, &s->z2, &s->h2, &s->z3, &s->h3, &s->dz, &s->dz2}) A((void**)p, N * CH * 2);
     A((void**)&s->o, N * 4); A((void**)&s->dO, N * 4);
-    A((void**)&s->sums, sizeof(double) * 2 * 64 * batch_max);
+    A((void**)&s->sums, sizeof(double) * (2 * L4_MAXBLK + 1) * batch_max);  // partials + corrections
     A((void**)&s->partial, sizeof(float) * (size_t)cgmax * 9216 + sizeof(float) * 320 * cgmax);
     A((void**)&s->lpart, sizeof(double) * s->nsm * 8);
     A((void**)&s->thin_out, sizeof(float) * 320);
@@ -744,7 +1051,7 @@ int phix_surrogate_get_params(phix_surrogate_t* s, float* host_params, float* ho
 // c_out = projection(c + out_scale * net(c)); c, c_out: [B][H][W] FP64 device.
 int phix_surrogate_step(phix_surrogate_t* s, const double* c, double* c_out, int B, void* stream) {
     if (!s || !c || !c_out || B < 1 || B > s->bmax) { set_error("surrogate_step: bad argument"); return PHIX_ERR_ARG; }
-    return sg_forward(s, c, B, c_out, nullptr, (cudaStream_t)stream);
+    return sg_forward(s, c, B, c_out, nullptr, (cudaStream_t)stream, false);
 }
 
 // Network output o (no update) for tests: o [B][H][W] FP32 device; also leaves
