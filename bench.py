@@ -188,7 +188,14 @@ class BatchRun:
 
     def __init__(self, px, torch, dev, args):
         from phix_b200 import workloads
-        grids, phys, prms, scheme, dt, _, fields = workloads.ch2d_batch()
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        # N ranks: a job of N x 64 instances (the first 64 are the 1-GPU
+        # workload), bin-packed across the ranks; no collective on the data path
+        grids, phys, prms, scheme, dt, _, fields = workloads.ch2d_batch(ninst=64 * world)
+        if world > 1:
+            mine = workloads.partition_instances([g.n[0] * g.n[1] for g in grids], world)[rank]
+            grids, prms, fields = [grids[i] for i in mine], [prms[i] for i in mine], [fields[i] for i in mine]
         self.K = 20
         self.prec = px.F64 if args.dtype == "f64" else px.F32
         w = 8 if self.prec == px.F64 else 4
@@ -284,7 +291,12 @@ def bench_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
-    value = world * run.cells * K * args.steps / (total_ms / 1e3)
+    job_cells = run.cells
+    if world > 1:
+        t = torch.tensor([float(run.cells)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        job_cells = float(t.item())
+    value = job_cells * K * args.steps / (total_ms / 1e3)
 
     # roofline: algorithmic bytes of one time step (13w per field-cell for RK4,
     # the traffic of one launch per stage; 2w for Euler) over the device time
@@ -330,7 +342,7 @@ def bench_ours(args):
         t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_value = world * run.cells * K * e2e_steps / (e2e_ms / 1e3)
+    e2e_value = job_cells * K * e2e_steps / (e2e_ms / 1e3)
 
     line = None
     if rank == 0:
@@ -368,7 +380,8 @@ def bench_ours(args):
                        else "FP32 stencils, compensated FP32 state, FP64 reductions",
                        "l2": "flushed between timed steps (256 MiB write); within a step the fields may stay "
                              "L2-resident",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": (f"instances bin-packed over {world} ranks" if args.workload == "batch"
+                                       else f"replicas x{world}")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": TRAFFIC.get((args.workload, args.dtype, run.lps)),
                          "note": f"algorithmic {per_cell} B per field-cell update over the CUDA-event time of "
@@ -386,6 +399,96 @@ def bench_ours(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    return line
+
+
+def bench_surrogate(args):
+    """Config 5: the learned CH 512^2 surrogate (committed parameters) against
+    the fused FD solver advancing the same simulated time.  One bench step =
+    SUR_K surrogate steps (SUR_K * 50 FD steps of simulated time, batch 1, with
+    the exact mass projection), timed with CUDA events; the FD legs run the
+    same simulated time in FP32 and FP64 (CUDA graphs of 50 steps)."""
+    import torch
+
+    import phix_b200 as px
+    from phix_b200 import surrogate as S
+    SUR_K = 40
+    p = S.load_params()
+    n = S.N
+    dev = torch.device("cuda", 0)
+    c0 = S.initial_field(100, n)
+    sg = px.Surrogate(n, n, 1, S.IN_SHIFT, S.IN_SCALE, S.OUT_SCALE)
+    sg.set_params(p)
+    a = torch.from_numpy(c0.copy()).to(dev)[None]
+    b = torch.empty_like(a)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        for _ in range(SUR_K):
+            sg.step(a, b)
+            a, b = b, a
+        flush_l2(flush)
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = px.launch_count()
+    with ClockSampler(dev.index) as clk:
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            for _ in range(SUR_K):
+                sg.step(a, b, stream)
+                a, b = b, a
+            ev[i][1].record(stream)
+            flush_l2(flush)
+        torch.cuda.synchronize(dev)
+    launches = px.launch_count() - launches0
+    total_ms = sum(s_.elapsed_time(e_) for s_, e_ in ev)
+    ms_per_step = total_ms / args.steps
+    sim_per_step = SUR_K * S.STEPS_PER_CALL * S.DT
+    value = sim_per_step / (ms_per_step / 1e3)
+    # e2e: host c -> device, SUR_K steps, device -> host, every step
+    h_in = torch.from_numpy(c0.copy())[None].pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    t0 = time.perf_counter()
+    for _ in range(max(3, args.steps // 2)):
+        a.copy_(h_in, non_blocking=True)
+        for _ in range(SUR_K):
+            sg.step(a, b, stream)
+            a, b = b, a
+        h_out.copy_(a, non_blocking=True)
+        torch.cuda.synchronize(dev)
+    e2e_ms = 1e3 * (time.perf_counter() - t0) / max(3, args.steps // 2)
+    sg.close()
+    fd = S.time_speed(p, sur_steps=SUR_K)
+    flops = 2 * 9 * (32 + 32 * 32 + 32 * 32 + 32) * n * n  # per surrogate step
+    achieved = flops * SUR_K / (ms_per_step / 1e3) / 1e12
+    peak = None
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        with open(pk) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+    line = {
+        "metric": "surrogate vs FD sim-time/s (CH 512^2, one surrogate step = 50 FD steps)",
+        "value": value, "unit": "simulated time units/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 activations, fp32 accumulate, fp64 state",
+        "data": "synthetic: c0 = U[0.35,0.65] mean + U[-0.01,0.01], numpy default_rng(100); "
+                "parameters trained on FD trajectories of seeds 100-299",
+        "config": {"workload": "CH 512^2 periodic surrogate rollout, batch 1", "surrogate_steps_per_step": SUR_K,
+                   "l2": "flushed between timed steps"},
+        "fd_comparison": {"fd_f32_sim_time_per_s": fd["sim_time"] / (fd["fd_f32_ms"] / 1e3),
+                          "fd_f64_sim_time_per_s": fd["sim_time"] / (fd["fd_f64_ms"] / 1e3),
+                          "speedup_vs_fd_f32": fd["fd_f32_ms"] / fd["surrogate_ms"],
+                          "speedup_vs_fd_f64": fd["fd_f64_ms"] / fd["surrogate_ms"]},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "note": "9.97 GFLOP per surrogate step (2*9*(32+1024+1024+32) per pixel) over the "
+                             "CUDA-event time of the whole step (all kernels); peak bf16_tflops measured"},
+        "e2e": {"value": sim_per_step / (e2e_ms / 1e3), "unit": "simulated time units/s",
+                "h2d_bytes_per_step": h_in.numel() * 8, "d2h_bytes_per_step": h_out.numel() * 8},
+        "gpu_launches": launches,
+        "clocks": clk.result,
+    }
+    print(json.dumps(line), flush=True)
     return line
 
 
@@ -463,8 +566,9 @@ def main():
     ap.add_argument("--n", type=int, default=1024, help="grid size n x n (the metric is quoted at 1024)")
     ap.add_argument("--cpu-baseline-steps", type=int, default=50)
     ap.add_argument("--ref-sample-steps", type=int, default=2)
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ch2d",
-                    help="ch2d: the headline CH 1024^2 case; ac2d, chac3d, batch: the other configurations")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["surrogate"], default="ch2d",
+                    help="ch2d: the headline CH 1024^2 case; ac2d, chac3d, batch, surrogate: the other "
+                         "configurations")
     ap.add_argument("--tiles", type=int, default=-1, help="2-D stage tile shape (phix_stepper_set_tiles)")
     ap.add_argument("--launch", choices=["auto", "step", "stage"], default="auto",
                     help="one launch per RK4 time step, one per stage, or the library default (auto)")
@@ -473,6 +577,8 @@ def main():
         args.warmup = max(args.warmup, 3)  # timing rule: at least 3 untimed warm-up steps
     if args.impl == "reference":
         bench_reference(args)
+    elif args.workload == "surrogate":
+        bench_surrogate(args)
     else:
         bench_ours(args)
 

@@ -85,14 +85,43 @@ def generate(seeds, nsteps: int, every: int = STEPS_PER_CALL, n: int = N, precis
     return data
 
 
+def shard_seeds(seeds, rank: int, world: int):
+    """Data-parallel training: rank r generates and trains on seeds r,
+    r+world, ...; every rank gets the same number (the remainder is dropped),
+    so all ranks take the same number of gradient all-reduces."""
+    seeds = list(seeds)
+    per = len(seeds) // world
+    return seeds[rank::world][:per]
+
+
+def allreduce_mean_(t, group=None):
+    """In-place mean of a gradient tensor over the ranks of `group`
+    (torch.distributed: NCCL between GPUs, gloo on CPU)."""
+    import torch.distributed as dist
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    t.div_(dist.get_world_size(group))
+    return t
+
+
+class _DeviceVector:
+    """A float32 device vector owned by the library, exposed to torch without a
+    copy through the CUDA array interface."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False), "version": 3}
+
+
 def train(seeds, nsteps: int = 40000, every: int = STEPS_PER_CALL, batch: int = 16, lr: float = 1e-3,
           chunk: int = 25, epochs: int = 1, lr_final: float = 1e-4, init_seed: int = 0, n: int = N, params=None,
-          log_every: int = 0, shuffle_seed: int = 0):
+          log_every: int = 0, shuffle_seed: int = 0, distributed: bool = False):
     """Train on FD trajectories generated chunk by chunk (`chunk` trajectories
     at a time, kept on the GPU): `epochs` passes over the chunk's shuffled
     (c_t, c_{t+every}) pairs per chunk, Adam with a learning rate decaying
-    geometrically from `lr` to `lr_final` over the whole run.  Returns (flat
-    params, log)."""
+    geometrically from `lr` to `lr_final` over the whole run.  With
+    `distributed` (an initialised torch.distributed NCCL group, one rank per
+    GPU) each rank takes its shard of the seeds and the gradients are averaged
+    over the ranks before every Adam step, so every rank holds the same
+    parameters.  Returns (flat params, log)."""
     import torch
     if params is None:
         params = init_params(init_seed)
@@ -100,6 +129,11 @@ def train(seeds, nsteps: int = 40000, every: int = STEPS_PER_CALL, batch: int = 
     sg.set_params(params)
     log = TrainLog()
     seeds = list(seeds)
+    grads = None
+    if distributed:
+        import torch.distributed as dist
+        seeds = shard_seeds(seeds, dist.get_rank(), dist.get_world_size())
+        grads = torch.as_tensor(_DeviceVector(sg.grad_ptr(), sg.nparams), device="cuda")
     rng = np.random.default_rng(shuffle_seed)
     ns = nsteps // every + 1
     total = max(1, (len(seeds) * (ns - 1) * epochs) // batch)
@@ -118,6 +152,8 @@ def train(seeds, nsteps: int = 40000, every: int = STEPS_PER_CALL, batch: int = 
                 a = data[ti, si].contiguous()
                 nxt = data[ti, si + 1].contiguous()
                 loss = sg.grad(a, nxt)
+                if grads is not None:
+                    allreduce_mean_(grads)
                 rate = lr * (lr_final / lr) ** min(1.0, log.updates / total)
                 sg.adam(rate)
                 log.updates += 1
@@ -376,12 +412,31 @@ def main(argv=None):
     ap.add_argument("--lr-final", type=float, default=1e-4)
     ap.add_argument("--chunk", type=int, default=25)
     ap.add_argument("--log-every", type=int, default=500)
+    ap.add_argument("--distributed", action="store_true",
+                    help="data-parallel training under torchrun (one rank per GPU, NCCL gradient averaging)")
     args = ap.parse_args(argv)
     lo, hi = (int(v) for v in args.seeds.split(":"))
     elo, ehi = (int(v) for v in args.eval_seeds.split(":"))
     if args.cmd == "train":
+        rank = 0
+        if args.distributed:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            local = int(os.environ.get("LOCAL_RANK", "0"))
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+            rank = dist.get_rank()
         p, log = train(range(lo, hi), nsteps=args.nsteps, batch=args.batch, lr=args.lr, lr_final=args.lr_final,
-                       chunk=args.chunk, epochs=args.epochs, log_every=args.log_every)
+                       chunk=args.chunk, epochs=args.epochs, log_every=args.log_every if rank == 0 else 0,
+                       distributed=args.distributed)
+        if args.distributed:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank != 0:
+            return
         np.savez(args.params, params=p, seeds=np.arange(lo, hi), nsteps=args.nsteps, epochs=args.epochs,
                  losses=np.asarray(log.losses[::10], np.float32))
         print(json.dumps({"updates": log.updates, "pairs": log.pairs, "seconds_fd": log.seconds_fd,

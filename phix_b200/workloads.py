@@ -70,3 +70,17 @@ def ch2d_batch(ninst=64, seed=3, nsteps=5000, dt=0.005, sizes=BATCH_SIZES):
         prms.append([M, kappa, 1.0, 0.0, 1.0])
         fields.append(_stored(g, c))
     return grids, PHYS_CH, prms, RK4, dt, nsteps, fields
+
+
+def partition_instances(costs, world: int):
+    """Greedy bin-pack of independent instances onto `world` ranks: instances
+    in decreasing cost (ties by index) go to the least-loaded rank (ties by
+    rank).  Returns one list of instance indices per rank, each ascending."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]
