@@ -131,9 +131,13 @@ WORKLOADS = {
               "synthetic: per-instance size/kappa/M/mean from numpy default_rng(3)"),
 }
 
-# DRAM bytes (read + write) per time step, from the ncu captures summarised
-# under profiles/; keyed by (workload, dtype, launches per time step).
-TRAFFIC = {}
+# DRAM bytes (read + write) per launch of the dominant kernel, from the ncu
+# captures summarised under profiles/ (cold L2, so an upper bound for the
+# graph-replayed launches); keyed by (workload, dtype, launches per time step).
+TRAFFIC = {
+    ("ch2d", "f64", 4): 12.63e6,  # profiles/stage_box_ch1024_f64.md: mean of stage 1 and 2 launches
+    ("ch2d", "f32", 1): 8.47e6,   # profiles/step_box_ch1024_f32.md
+}
 
 
 class StepperRun:
@@ -386,7 +390,8 @@ def bench_ours(args):
                          "frac": achieved / peak, "traffic": TRAFFIC.get((args.workload, args.dtype, run.lps)),
                          "note": f"algorithmic {per_cell} B per field-cell update over the CUDA-event time of "
                                  f"one time step ({run.lps} launch{'es' if run.lps > 1 else ''} per time step); "
-                                 f"peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+                                 f"peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs); traffic = ncu DRAM bytes per "
+                                 f"launch of the dominant kernel (bytes, cold L2)"},
             "hbm_gbs_effective": achieved,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": run.io_bytes,

@@ -401,7 +401,9 @@ def main(argv=None):
     import argparse
     import json
     ap = argparse.ArgumentParser(description="train / evaluate / time the CH 512^2 surrogate")
-    ap.add_argument("cmd", choices=["train", "evaluate", "time"])
+    ap.add_argument("cmd", choices=["train", "evaluate", "time", "rollout"])
+    ap.add_argument("--steps", type=int, default=800, help="rollout: surrogate steps")
+    ap.add_argument("--recheck", type=int, default=10, help="rollout: FD re-check every this many steps")
     ap.add_argument("--params", default=PARAMS_FILE)
     ap.add_argument("--seeds", default="100:300", help="training seeds lo:hi")
     ap.add_argument("--eval-seeds", default="300:304")
@@ -447,6 +449,18 @@ def main(argv=None):
         if args.cmd == "evaluate":
             for r in evaluate(p, range(elo, ehi)):
                 print(json.dumps(r))
+        elif args.cmd == "rollout":
+            import torch
+            for sd in range(elo, ehi):
+                c0 = initial_field(sd)
+                out, rl = rollout(p, c0, args.steps, recheck=args.recheck)
+                ref, fd_s = fd_run(c0, args.steps * STEPS_PER_CALL, precision=F64)
+                a, r = torch.from_numpy(out), torch.from_numpy(ref)
+                print(json.dumps({"seed": sd, "steps": args.steps, "recheck": args.recheck, "rel_l2": _rel(a, r),
+                                  "rel_l2_fluct": _rel_fluct(a, r), "mass_rel": abs(float(out.mean() - c0.mean()))
+                                  / abs(float(c0.mean())), "surrogate_steps": rl.surrogate_steps,
+                                  "fd_takeovers": rl.fd_takeovers, "rechecks": rl.rechecks,
+                                  "rollout_s": rl.seconds, "fd_f64_s": fd_s}))
         else:
             print(json.dumps(time_speed(p)))
 
