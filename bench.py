@@ -210,8 +210,13 @@ class BatchRun:
         self.d = [torch.from_numpy(f).to(dev) for f in fields]
         for i, t in enumerate(self.d):
             self.b.load(i, t)
-        self.b.autotune(2)
-        self.lps = 4
+        if args.launch == "step":
+            self.b.set_fusion(True)
+        else:
+            self.b.autotune(2)  # tile shape, CTAs per SM, one launch per step or per stage
+            if args.launch == "stage":
+                self.b.set_fusion(False)
+        self.lps = self.b.launches_per_step
         self.b.set_graph(self.K)
         self.h_in = [torch.from_numpy(f).pin_memory() for f in fields]
         self.h_out = [torch.empty_like(h).pin_memory() for h in self.h_in]

@@ -23,6 +23,12 @@ namespace phix {
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* where);
 void count_launch(int n = 1);
+// While alive on this thread, launches are not counted (kernels recorded into
+// a graph under stream capture; the graph's replay counts them instead).
+struct LaunchCountPause {
+    LaunchCountPause();
+    ~LaunchCountPause();
+};
 
 #define PHIX_TRY_CUDA(call)                                  \
     do {                                                     \

@@ -179,17 +179,15 @@ __global__ void __launch_bounds__(NT) step_box(const StepArgs<T> A, const Pol po
     step_tile<T, Pol, TX, TY, NT>(A, pol, reinterpret_cast<T*>(step_smem), blockIdx.x * TX, blockIdx.y * TY);
 }
 
-// Many fields in one persistent launch (tile list as in stage_box_batched).
+// Many fields in one launch: one CTA per entry of the tile list (a persistent
+// loop over tiles makes ptxas spill this body heavily).
 template <typename T, class Pol, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT) step_box_batched(const StepArgs<T>* __restrict__ args,
-                                                       const BatchTile* __restrict__ tiles, int ntiles,
-                                                       const Pol pol) {
+                                                       const BatchTile* __restrict__ tiles, const Pol pol) {
     extern __shared__ __align__(16) unsigned char step_smem[];
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const BatchTile bt = tiles[t];
-        step_tile<T, Pol, TX, TY, NT>(args[bt.inst], pol, reinterpret_cast<T*>(step_smem), bt.x0, bt.y0);
-        __syncthreads();
-    }
+    const BatchTile bt = tiles[blockIdx.x];
+    const StepArgs<T> a = args[bt.inst];
+    step_tile<T, Pol, TX, TY, NT>(a, pol, reinterpret_cast<T*>(step_smem), bt.x0, bt.y0);
 }
 
 // True when the fused step supports this grid's boundaries (2-D, every side

@@ -166,10 +166,13 @@ int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step);
 /* Kernel launches one time step takes with the current settings. */
 int phix_stepper_launches_per_step(const phix_stepper_t* h);
 
-/* Tile shape of the 2-D per-stage kernels: -1 the box tiles (64x16, 256
- * threads, flat cell loops), 0..3 column-walking tiles (TX x TY = 64x16,
- * 64x32, 128x16, 32x16 with 4, 4, 2, 8 row groups; 256 threads).  All give the
- * same bits.  No reference counterpart. */
+/* Tile shape of the 2-D kernels.  One launch per stage: -1 the box tiles
+ * (64x16, 256 threads, flat cell loops), 0..3 column-walking tiles (TX x TY =
+ * 64x16, 64x32, 128x16, 32x16 with 4, 4, 2, 8 row groups; 256 threads).  One
+ * launch per RK4 step: 0..5 tiles of 64x16, 64x32, 128x16, 128x32 (512
+ * threads), 128x64 and 256x32 (1024 threads; FP32 only, where they fit in
+ * shared memory); -1 picks 128x64 for FP32 grids of at most one wave of such
+ * tiles, else 128x32.  All give the same bits.  No reference counterpart. */
 int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg);
 
 /* FP64 only: run directly on caller-owned buffers, no copies.  fields[f] is
@@ -190,13 +193,25 @@ typedef struct phix_batch phix_batch_t;
 
 /* ninst independent 2-D simulations of one single-field physics (AC or CH),
  * each with its own grid (size, spacing, BCs) and its own prm[8*i .. 8*i+7],
- * advanced in lockstep with time step dt.  Each RK stage of all instances is
- * one persistent kernel over a shared tile list; state and stage buffers come
- * from one device pool.  No reference counterpart: the reference runs one
+ * advanced in lockstep with time step dt.  Each RK4 step of all instances is
+ * one launch (phix_batch_set_fusion), else each stage is one persistent
+ * kernel over a shared tile list; state and stage buffers come from one
+ * device pool.  No reference counterpart: the reference runs one
  * Solver per field (Solver.cu:86-107), i.e. instances one after another. */
 int phix_batch_create(phix_batch_t** out, int phys, int scheme, int precision, int ninst, const phix_grid_t* grids,
                       const double* prm, double dt);
 int phix_batch_destroy(phix_batch_t* b);
+
+/* 1: run each RK4 step of the whole batch as one launch (one CTA per 128x32
+ * tile, the four stage states in shared memory, tile halos recomputed);
+ * needs RK4 and periodic or zero-flux sides on every instance, else
+ * PHIX_ERR_UNSUPPORTED.  0: one launch per stage.  Both give the same bits.
+ * Default: 1 wherever it is possible (the faster on B200 in both
+ * precisions).  No reference counterpart. */
+int phix_batch_set_fusion(phix_batch_t* b, int one_launch_per_step);
+
+/* Kernel launches one batched time step takes with the current settings. */
+int phix_batch_launches_per_step(const phix_batch_t* b);
 /* Copy one instance's FP64 stored array in / out (device, or host when
  * from_host / to_host is non-zero; host copies are synchronous). */
 int phix_batch_load(phix_batch_t* b, int inst, const double* field, int from_host, void* stream);
@@ -207,8 +222,9 @@ int phix_batch_set_graph(phix_batch_t* b, int steps_per_graph);
  * CTAs per SM of the persistent launches (0 = occupancy limit). */
 int phix_batch_set_tiles(phix_batch_t* b, int tile_cfg, int ctas_per_sm);
 int phix_batch_get_tiles(const phix_batch_t* b, int* tile_cfg, int* ctas_per_sm, int* ntiles);
-/* Time every tile shape x CTA count on trial_steps steps of the real batch
- * (state saved and restored), keep the fastest; *best_ms = ms per step. */
+/* Time every tile shape x CTA count of the one-launch-per-stage kernels, and
+ * the one-launch step where possible, on trial_steps steps of the real batch
+ * (state saved and restored); keep the fastest; *best_ms = ms per step. */
 int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms);
 /* FP64 mass (sum of u * dV over physical cells) per instance; synchronous. */
 int phix_batch_mass(phix_batch_t* b, double* masses);

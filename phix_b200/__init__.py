@@ -114,6 +114,8 @@ def lib() -> C.CDLL:
         "phix_reduce_mass_energy_noalloc": ([C.POINTER(vp), C.c_int, P, G, P, vp], C.c_int),
         "phix_batch_create": ([C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_int, G, P, C.c_double], C.c_int),
         "phix_batch_destroy": ([vp], C.c_int),
+        "phix_batch_launches_per_step": ([vp], C.c_int),
+        "phix_batch_set_fusion": ([vp, C.c_int], C.c_int),
         "phix_batch_load": ([vp, C.c_int, vp, C.c_int, vp], C.c_int),
         "phix_batch_store": ([vp, C.c_int, vp, C.c_int, vp], C.c_int),
         "phix_batch_advance": ([vp, C.c_int, vp], C.c_int),
@@ -364,6 +366,14 @@ class Batch:
 
     def set_graph(self, steps: int):
         check(lib().phix_batch_set_graph(self.h, steps))
+
+    def set_fusion(self, on: bool):
+        """One launch per RK4 step for the whole batch (True) or one per stage."""
+        check(lib().phix_batch_set_fusion(self.h, 1 if on else 0))
+
+    @property
+    def launches_per_step(self) -> int:
+        return lib().phix_batch_launches_per_step(self.h)
 
     def set_tiles(self, cfg: int, ctas_per_sm: int = 0):
         check(lib().phix_batch_set_tiles(self.h, cfg, ctas_per_sm))

@@ -16,6 +16,7 @@
 
 #include "phix/detail/common.cuh"
 #include "phix/detail/stage.cuh"
+#include "phix/detail/step2d.cuh"
 #include "stepper.h"
 
 namespace phix {
@@ -41,6 +42,39 @@ int launch_batched_cfg(const StageArgs<T>* args, const BatchTile* tiles, int nti
     kern<<<grid, NT, 0, s>>>(args, tiles, ntiles, Pol{});
     PHIX_LAUNCH_CHECK("stage_box_batched");
     return PHIX_OK;
+}
+
+// One launch per RK4 step over the whole batch (step2d.cuh): 128x32 tiles,
+// 512 threads, one CTA per tile of the step tile list.
+constexpr int BST_TX = 128, BST_TY = 32, BST_NT = 512;
+
+template <typename T, int PHYS>
+int batched_step_cfg(bool prepare, const StepArgs<T>* args, const BatchTile* tiles, int ntiles, int nsm,
+                     cudaStream_t s) {
+    using Pol = typename PolOf<PHYS>::type;
+    using G = Step2D<T, Pol, BST_TX, BST_TY>;
+    auto kern = step_box_batched<T, Pol, BST_TX, BST_TY, BST_NT>;
+    if (G::smem_bytes() > 227 * 1024) {
+        if (prepare) return PHIX_OK;
+        set_error("batch: the one-launch step tile does not fit in shared memory");
+        return PHIX_ERR_UNSUPPORTED;
+    }
+    if (prepare) {
+        PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
+        return PHIX_OK;
+    }
+    (void)nsm;
+    if (ntiles < 1) return PHIX_OK;
+    kern<<<ntiles, BST_NT, G::smem_bytes(), s>>>(args, tiles, Pol{});
+    PHIX_LAUNCH_CHECK("step_box_batched");
+    return PHIX_OK;
+}
+
+template <typename T>
+int batched_step(int phys, bool prepare, const StepArgs<T>* args, const BatchTile* tiles, int ntiles, int nsm,
+                 cudaStream_t s) {
+    if (phys == PHIX_PHYS_AC) return batched_step_cfg<T, PHIX_PHYS_AC>(prepare, args, tiles, ntiles, nsm, s);
+    return batched_step_cfg<T, PHIX_PHYS_CH>(prepare, args, tiles, ntiles, nsm, s);
 }
 
 template <typename T, int PHYS, int MODE>
@@ -147,6 +181,11 @@ struct phix_batch {
     cudaStream_t cap = nullptr;
     int graph_steps = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    // one launch per RK4 step (possible where every side is periodic or zero-flux)
+    bool can_fuse = false, fuse_steps = false;
+    void* step_args_dev = nullptr;  // [parity][ninst] StepArgs
+    BatchTile* step_tiles_dev = nullptr;
+    int step_ntiles = 0;
 };
 
 namespace phix {
@@ -255,11 +294,54 @@ int build_args(phix_batch* b) {
     return PHIX_OK;
 }
 
+// StepArgs per parity and instance, and the tile list of the step kernel.
+template <typename T>
+int build_step(phix_batch* b) {
+    std::vector<StepArgs<T>> h((size_t)2 * b->ninst);
+    memset(h.data(), 0, sizeof(StepArgs<T>) * h.size());
+    for (int par = 0; par < 2; ++par)
+        for (int i = 0; i < b->ninst; ++i) {
+            StepArgs<T>& B = h[(size_t)par * b->ninst + i];
+            const phix_grid_t& g = b->grids[i];
+            B.S.L = b->layouts[i];
+            for (int a = 0; a < 3; ++a) B.S.i2[a] = a < g.dim ? (T)(1.0 / (g.d[a] * g.d[a])) : (T)0;
+            make_coeffs<T>(b->phys, &b->prm[8 * i], B.S.p);
+            B.S.u[0] = (const T*)b->st[par][i];
+            B.S.out[0] = (T*)b->st[1 - par][i];
+            B.S.dtf = (T)(b->dt / 6.0);
+            if (b->lo[0][i]) {
+                B.S.ulo[0] = (const T*)b->lo[par][i];
+                B.S.outlo[0] = (T*)b->lo[1 - par][i];
+            }
+            B.dt2 = (T)(b->dt * 0.5);
+            B.dt = (T)b->dt;
+        }
+    PHIX_TRY_CUDA(cudaMalloc(&b->step_args_dev, sizeof(StepArgs<T>) * h.size()));
+    PHIX_TRY_CUDA(cudaMemcpy(b->step_args_dev, h.data(), sizeof(StepArgs<T>) * h.size(), cudaMemcpyHostToDevice));
+    // tiles, largest instances first (the persistent walk stays balanced)
+    std::vector<int> order(b->ninst);
+    for (int i = 0; i < b->ninst; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        return (long long)b->grids[a].n[0] * b->grids[a].n[1] > (long long)b->grids[c].n[0] * b->grids[c].n[1];
+    });
+    std::vector<BatchTile> tiles;
+    for (int i : order)
+        for (int y = 0; y < b->grids[i].n[1]; y += BST_TY)
+            for (int x = 0; x < b->grids[i].n[0]; x += BST_TX) tiles.push_back({i, x, y, 0});
+    b->step_ntiles = (int)tiles.size();
+    PHIX_TRY_CUDA(cudaMalloc(&b->step_tiles_dev, sizeof(BatchTile) * tiles.size()));
+    PHIX_TRY_CUDA(cudaMemcpy(b->step_tiles_dev, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice));
+    return batched_step<T>(b->phys, true, nullptr, nullptr, 0, 0, nullptr);
+}
+
 template <typename T>
 int batch_step(phix_batch* b, cudaStream_t s) {
     const int par = b->cur;
     int rc;
-    if (b->scheme == PHIX_EULER) {
+    if (b->fuse_steps) {
+        const StepArgs<T>* args = reinterpret_cast<const StepArgs<T>*>(b->step_args_dev) + (size_t)par * b->ninst;
+        if ((rc = batched_step<T>(b->phys, false, args, b->step_tiles_dev, b->step_ntiles, b->nsm, s))) return rc;
+    } else if (b->scheme == PHIX_EULER) {
         rc = launch_batched<T>(b->phys, MODE_EULER_FINAL, b->cfg, args_table<T>(b, 4, par), b->tiles_dev, b->ntiles,
                                b->ctas_per_sm, b->nsm, s);
         if (rc) return rc;
@@ -289,7 +371,11 @@ int batch_replay(phix_batch* b, cudaStream_t s) {
     if (!b->gexec[parity]) {
         cudaGraph_t graph = nullptr;
         PHIX_TRY_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
-        int rc = batch_steps(b, b->graph_steps, b->cap);
+        int rc;
+        {
+            LaunchCountPause pause;  // recorded, not launched: the replay below counts them
+            rc = batch_steps(b, b->graph_steps, b->cap);
+        }
         cudaError_t e = cudaStreamEndCapture(b->cap, &graph);
         b->cur = parity;
         if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
@@ -299,7 +385,7 @@ int batch_replay(phix_batch* b, cudaStream_t s) {
         if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
     }
     PHIX_TRY_CUDA(cudaGraphLaunch(b->gexec[parity], s));
-    count_launch(b->graph_steps * (b->scheme == PHIX_RK4 ? 4 : 1));
+    count_launch(b->graph_steps * (b->scheme == PHIX_RK4 && !b->fuse_steps ? 4 : 1));
     if (b->graph_steps % 2) b->cur = 1 - parity;
     return PHIX_OK;
 }
@@ -370,6 +456,14 @@ int phix_batch_create(phix_batch_t** out, int phys, int scheme, int precision, i
     cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev);
     int rc = b->prec == PHIX_F32 ? build_args<float>(b) : build_args<double>(b);
     if (!rc) rc = build_tiles(b, 0);
+    // one launch per RK4 step: available, and the default, for batches whose
+    // sides are all periodic or zero-flux (phix_batch_set_fusion)
+    bool steppable = scheme == PHIX_RK4;
+    for (int i = 0; i < ninst && steppable; ++i) steppable = step2d_supported(b->layouts[i], grids[i].dim);
+    if (!rc && steppable) {
+        rc = b->prec == PHIX_F32 ? build_step<float>(b) : build_step<double>(b);
+        b->can_fuse = b->fuse_steps = rc == PHIX_OK;
+    }
     if (!rc) {
         std::vector<double> dv(ninst, 1.0);
         for (int i = 0; i < ninst; ++i)
@@ -385,6 +479,11 @@ int phix_batch_create(phix_batch_t** out, int phys, int scheme, int precision, i
     return PHIX_OK;
 }
 
+int phix_batch_launches_per_step(const phix_batch_t* b) {
+    if (!b) return -1;
+    return b->scheme == PHIX_RK4 && !b->fuse_steps ? 4 : 1;
+}
+
 int phix_batch_destroy(phix_batch_t* b) {
     if (!b) return PHIX_OK;
     batch_drop_graphs(b);
@@ -395,6 +494,8 @@ int phix_batch_destroy(phix_batch_t* b) {
     if (b->part_dev) cudaFree(b->part_dev);
     if (b->dv_dev) cudaFree(b->dv_dev);
     if (b->mass_dev) cudaFree(b->mass_dev);
+    if (b->step_args_dev) cudaFree(b->step_args_dev);
+    if (b->step_tiles_dev) cudaFree(b->step_tiles_dev);
     if (b->cap) cudaStreamDestroy(b->cap);
     delete b;
     return PHIX_OK;
@@ -470,6 +571,20 @@ int phix_batch_get_tiles(const phix_batch_t* b, int* tile_cfg, int* ctas_per_sm,
     return PHIX_OK;
 }
 
+int phix_batch_set_fusion(phix_batch_t* b, int one_launch_per_step) {
+    if (!b) { set_error("batch_set_fusion: NULL batch"); return PHIX_ERR_ARG; }
+    const bool f = one_launch_per_step != 0;
+    if (f && !b->can_fuse) {
+        set_error("batch_set_fusion: one launch per step needs RK4 and periodic or zero-flux sides everywhere");
+        return PHIX_ERR_UNSUPPORTED;
+    }
+    if (f != b->fuse_steps) {
+        batch_drop_graphs(b);
+        b->fuse_steps = f;
+    }
+    return PHIX_OK;
+}
+
 int phix_batch_set_graph(phix_batch_t* b, int steps_per_graph) {
     if (!b || steps_per_graph < 0) { set_error("batch_set_graph: bad argument"); return PHIX_ERR_ARG; }
     batch_drop_graphs(b);
@@ -512,20 +627,35 @@ int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms) {
     cudaEventCreate(&e1);
     float best = 1e30f;
     int best_cfg = 0, best_cps = 0;
+    bool best_fused = false;
     const int cps_options[] = {0, 2, 4};
     int rc = PHIX_OK;
+    auto trial = [&](float* ms) {
+        int r = batch_steps(b, 1, 0);  // warm-up
+        if (r) return r;
+        cudaEventRecord(e0, 0);
+        if ((r = batch_steps(b, trial_steps, 0))) return r;
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(ms, e0, e1);
+        return PHIX_OK;
+    };
+    // one launch per stage: every tile shape x CTA count
+    b->fuse_steps = false;
     for (int cfg = 0; cfg < kNumTileCfgs && !rc; ++cfg) {
         for (int cps : cps_options) {
-            if ((rc = phix_batch_set_tiles(b, cfg, cps))) break;
-            if ((rc = batch_steps(b, 1, 0))) break;  // warm-up
-            cudaEventRecord(e0, 0);
-            if ((rc = batch_steps(b, trial_steps, 0))) break;
-            cudaEventRecord(e1, 0);
-            cudaEventSynchronize(e1);
             float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
+            if ((rc = phix_batch_set_tiles(b, cfg, cps)) || (rc = trial(&ms))) break;
             if (ms < best) { best = ms; best_cfg = cfg; best_cps = cps; }
         }
+    }
+    // one launch per RK4 step
+    if (!rc && b->can_fuse) {
+        float ms = 0.f;
+        b->fuse_steps = true;
+        rc = trial(&ms);
+        b->fuse_steps = false;
+        if (!rc && ms < best) { best = ms; best_fused = true; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -542,6 +672,7 @@ int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms) {
     b->graph_steps = old_graph;
     if (rc) return rc;
     rc = phix_batch_set_tiles(b, best_cfg, best_cps);
+    if (!rc) rc = phix_batch_set_fusion(b, best_fused ? 1 : 0);
     if (best_ms) *best_ms = best / trial_steps;
     return rc;
 }

@@ -23,7 +23,13 @@ int cuda_status(cudaError_t e, const char* where) {
     return PHIX_ERR_CUDA;
 }
 
-void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+static thread_local int t_count_paused = 0;
+
+void count_launch(int n) {
+    if (!t_count_paused) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+LaunchCountPause::LaunchCountPause() { ++t_count_paused; }
+LaunchCountPause::~LaunchCountPause() { --t_count_paused; }
 
 }  // namespace phix
 

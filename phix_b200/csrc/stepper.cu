@@ -155,24 +155,55 @@ int launch_mode(int dim, int mode, const StageArgs<T>& A, cudaStream_t s, int ti
 // ---------------------------------------------------------------------------
 // one launch per RK4 step (2-D, one field)
 // ---------------------------------------------------------------------------
-constexpr int ST_TX = 64, ST_TY = 16, ST_NT = 256;
+// tiles of the one-launch step: (TX, TY, threads); index 0 is the default
+constexpr int kStepCfgs[][3] = {{64, 16, 256}, {64, 32, 256}, {128, 16, 256}, {128, 32, 512}, {128, 64, 1024},
+                                 {256, 32, 1024}};
+constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100
+constexpr int kNumStepCfgs = sizeof(kStepCfgs) / sizeof(kStepCfgs[0]);
 
-template <typename T, int PHYS>
-int prepare_step2d_t() {
-    using Pol = typename PolOf<PHYS>::type;
-    using G = Step2D<T, Pol, ST_TX, ST_TY>;
-    PHIX_TRY_CUDA(cudaFuncSetAttribute(step_box<T, Pol, ST_TX, ST_TY, ST_NT>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
+template <typename T, class Pol, int TX, int TY, int NT>
+int step_cfg(bool prepare, const StepArgs<T>* A, cudaStream_t s) {
+    using G = Step2D<T, Pol, TX, TY>;
+    if (G::smem_bytes() > kMaxSmem) {  // this tile does not fit for this type / physics
+        if (prepare) return PHIX_OK;
+        set_error("step2d: a %dx%d tile needs %zu bytes of shared memory", TX, TY, G::smem_bytes());
+        return PHIX_ERR_UNSUPPORTED;
+    }
+    if (prepare) {
+        PHIX_TRY_CUDA(cudaFuncSetAttribute(step_box<T, Pol, TX, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)G::smem_bytes()));
+        return PHIX_OK;
+    }
+    dim3 grid((A->S.L.n[0] + TX - 1) / TX, (A->S.L.n[1] + TY - 1) / TY, 1);
+    step_box<T, Pol, TX, TY, NT><<<grid, NT, G::smem_bytes(), s>>>(*A, Pol{});
+    PHIX_LAUNCH_CHECK("step_box");
     return PHIX_OK;
 }
 
 template <typename T, int PHYS>
-int launch_step2d_t(const StepArgs<T>& A, cudaStream_t s) {
+int step_dispatch(int cfg, bool prepare, const StepArgs<T>* A, cudaStream_t s) {
     using Pol = typename PolOf<PHYS>::type;
-    using G = Step2D<T, Pol, ST_TX, ST_TY>;
-    dim3 grid((A.S.L.n[0] + ST_TX - 1) / ST_TX, (A.S.L.n[1] + ST_TY - 1) / ST_TY, 1);
-    step_box<T, Pol, ST_TX, ST_TY, ST_NT><<<grid, ST_NT, G::smem_bytes(), s>>>(A, Pol{});
-    PHIX_LAUNCH_CHECK("step_box");
+    switch (cfg) {
+#define PHIX_STEP_CASE(i) \
+    case i: return step_cfg<T, Pol, kStepCfgs[i][0], kStepCfgs[i][1], kStepCfgs[i][2]>(prepare, A, s);
+        PHIX_STEP_CASE(0)
+        PHIX_STEP_CASE(1)
+        PHIX_STEP_CASE(2)
+        PHIX_STEP_CASE(3)
+        PHIX_STEP_CASE(4)
+        PHIX_STEP_CASE(5)
+#undef PHIX_STEP_CASE
+    }
+    set_error("step2d: bad tile configuration %d", cfg);
+    return PHIX_ERR_ARG;
+}
+
+template <typename T, int PHYS>
+int prepare_step2d_t() {
+    for (int c = 0; c < kNumStepCfgs; ++c) {
+        int rc = step_dispatch<T, PHYS>(c, true, nullptr, 0);
+        if (rc) return rc;
+    }
     return PHIX_OK;
 }
 
@@ -214,10 +245,29 @@ int prepare_stage(int phys, int dim, int prec) {
     return prec == PHIX_F32 ? prepare_t<float>(phys) : prepare_t<double>(phys);
 }
 
+// Default tile of the one-launch step (measured on B200): 128x32 with 512
+// threads, or 128x64 with 1024 threads in FP32 when those tiles fill at most
+// one wave (one CTA per SM: the smaller grids, e.g. 1024^2).
 template <typename T>
-int launch_step2d(int phys, const StepArgs<T>& A, cudaStream_t s) {
-    if (phys == PHIX_PHYS_AC) return launch_step2d_t<T, PHIX_PHYS_AC>(A, s);
-    if (phys == PHIX_PHYS_CH) return launch_step2d_t<T, PHIX_PHYS_CH>(A, s);
+int default_step_cfg(const Layout& L) {
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
+    }
+    if (sizeof(T) == 4) {
+        const long long tiles = (long long)((L.n[0] + 127) / 128) * ((L.n[1] + 63) / 64);
+        if (tiles <= nsm) return 4;
+    }
+    return 3;
+}
+
+template <typename T>
+int launch_step2d(int phys, const StepArgs<T>& A, cudaStream_t s, int tile) {
+    const int cfg = tile < 0 ? default_step_cfg<T>(A.S.L) : tile;
+    if (phys == PHIX_PHYS_AC) return step_dispatch<T, PHIX_PHYS_AC>(cfg, false, &A, s);
+    if (phys == PHIX_PHYS_CH) return step_dispatch<T, PHIX_PHYS_CH>(cfg, false, &A, s);
     set_error("step2d: physics %d has more than one field", phys);
     return PHIX_ERR_UNSUPPORTED;
 }
@@ -396,7 +446,7 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
         B.S = A;
         B.dt2 = (T)(h->dt * 0.5);
         B.dt = (T)h->dt;
-        if ((rc = launch_step2d<T>(h->phys, B, s))) return rc;
+        if ((rc = launch_step2d<T>(h->phys, B, s, h->tile))) return rc;
     } else {
         const T dt2 = (T)(h->dt * 0.5), dtt = (T)h->dt;
         // stage 1
@@ -440,7 +490,11 @@ static int replay_group(phix_stepper* h, cudaStream_t s) {
     if (!h->gexec[parity]) {
         cudaGraph_t graph = nullptr;
         PHIX_TRY_CUDA(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
-        int rc = enqueue_steps(h, h->graph_steps, h->cap);
+        int rc;
+        {
+            LaunchCountPause pause;  // recorded, not launched: the replay below counts them
+            rc = enqueue_steps(h, h->graph_steps, h->cap);
+        }
         cudaError_t e = cudaStreamEndCapture(h->cap, &graph);
         if (rc) { if (graph) cudaGraphDestroy(graph); h->cur = parity; return rc; }
         if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
@@ -576,7 +630,10 @@ int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step) {
 int phix_stepper_launches_per_step(const phix_stepper_t* h) { return h ? launches_per_step(h) : -1; }
 
 int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg) {
-    if (!h || tile_cfg < -1 || tile_cfg >= kNumColCfgs) { set_error("set_tiles: bad stepper or configuration"); return PHIX_ERR_ARG; }
+    if (!h || tile_cfg < -1 || tile_cfg >= (kNumColCfgs > kNumStepCfgs ? kNumColCfgs : kNumStepCfgs)) {
+        set_error("set_tiles: bad stepper or configuration");
+        return PHIX_ERR_ARG;
+    }
     if (tile_cfg != h->tile) {
         drop_graphs(h);
         h->tile = tile_cfg;

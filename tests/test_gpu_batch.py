@@ -43,6 +43,8 @@ def single(g, phys, prm, scheme, dt, field, nsteps, prec):
 def test_batch_matches_single_field_stepper(cuda, prec, cfg):
     grids, phys, prms, scheme, dt, fields = small_batch(prec)
     b = px.Batch(phys, scheme, prec, grids, prms, dt)
+    b.set_fusion(False)  # one launch per stage, with this tile shape
+    assert b.launches_per_step == 4
     b.set_tiles(cfg, 0)
     for i, f in enumerate(fields):
         b.load(i, f)
@@ -76,4 +78,46 @@ def test_batch_mass_and_autotune(cuda):
         ref, _ = px.reduce_mass_energy([d], phys, prms[i], g)
         assert abs(m0[i] - ref) <= 1e-6 * abs(ref)  # FP32 state vs FP64 input
         assert abs(m1[i] - m0[i]) <= 1e-5 * abs(m0[i])
+    b.close()
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32])
+@pytest.mark.parametrize("graph", [0, 3])
+def test_batch_one_launch_step_matches_single_field_stepper(cuda, prec, graph):
+    """One launch per RK4 step over the whole batch gives each instance the
+    bits of the single-field stepper."""
+    grids, phys, prms, scheme, dt, fields = small_batch(prec)
+    b = px.Batch(phys, scheme, prec, grids, prms, dt)
+    assert b.launches_per_step == 1  # the default where every side allows it
+    b.set_fusion(False)
+    assert b.launches_per_step == 4
+    b.set_fusion(True)
+    assert b.launches_per_step == 1
+    for i, f in enumerate(fields):
+        b.load(i, f)
+    b.set_graph(graph)
+    nsteps = 7
+    before = px.launch_count()
+    b.advance(nsteps)
+    torch.cuda.synchronize()
+    assert px.launch_count() - before == nsteps
+    for i, (g, prm, f) in enumerate(zip(grids, prms, fields)):
+        out = np.empty_like(f)
+        b.store(i, out)
+        want = single(g, phys, prm, scheme, dt, f, nsteps, prec)
+        gh = g.ghost
+        sl = (slice(gh, gh + g.n[2]), slice(gh, gh + g.n[1]), slice(gh, gh + g.n[0]))
+        assert np.array_equal(out[sl], want[sl]), i
+    b.close()
+
+
+def test_batch_one_launch_step_needs_periodic_or_noflux_sides(cuda):
+    grids, phys, prms, scheme, dt, fields = small_batch(px.F32)
+    grids[2] = px.make_grid((grids[2].n[0], grids[2].n[1]), bc=(px.BC_FIXED,) * 4 + (px.BC_PERIODIC,) * 2)
+    b = px.Batch(phys, scheme, px.F32, grids, prms, dt)
+    assert b.launches_per_step == 4
+    with pytest.raises(px.PhixError):
+        b.set_fusion(True)
+    b.set_fusion(False)
+    assert b.launches_per_step == 4
     b.close()

@@ -309,3 +309,37 @@ def test_stage_tile_shapes_give_identical_bits(cuda, oracle, prec, case):
         oracle.advance(want, phys, prm, px.RK4, dt, 6, grid, fma_mode=1)
         for a, b in zip(outs[0], want):
             assert np.array_equal(a[keep], b[keep]), _where(a, b, keep)
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32])
+@pytest.mark.parametrize("case", [0, 1, 5])
+def test_one_launch_step_tile_shapes(cuda, prec, case):
+    """Every tile shape of the one-launch RK4 step gives the per-stage bits."""
+    phys, n, bx, by, d = FUSED_CASES[case]
+    bcs = (bx, bx, by, by, 0, 0)
+    g = px.make_grid(n, d, 1, bcs)
+    grid = Grid(n=n, d=d, bc=bcs, bc_val=(0,) * 6)
+    rng = np.random.default_rng(300 + case)
+    lo_hi = (0.3, 0.7) if phys == px.PHYS_CH else (-0.6, 0.6)
+    x = grid.stored_from_phys(rng.uniform(*lo_hi, size=(1, n[1], n[0])))
+    prm = [1.0, 0.6, 1.2, 0.05, 0.95] if phys == px.PHYS_CH else [0.8, 1.3]
+    dt = 0.004 if phys == px.PHYS_CH else 0.02
+    outs = {}
+    tiles = ((False, -1), (True, -1), (True, 0), (True, 1), (True, 2), (True, 3))
+    if prec == px.F32:
+        tiles += ((True, 4), (True, 5))
+    for fused, tile in tiles:
+        st = px.Stepper(phys, px.RK4, prec, prm, dt, g)
+        st.set_fusion(fused)
+        st.set_tiles(tile)
+        t = torch.from_numpy(x.copy()).cuda()
+        st.load([t])
+        st.advance(7)
+        st.store([t])
+        torch.cuda.synchronize()
+        st.close()
+        outs[(fused, tile)] = t.cpu().numpy()
+    keep = ~corner_mask(grid)
+    base = outs[(False, -1)]
+    for key, a in outs.items():
+        assert np.array_equal(a[keep], base[keep]), (key, _where(a, base, keep))
