@@ -165,9 +165,13 @@ class StepperRun:
         if args.launch != "auto":
             self.st.set_fusion(args.launch == "step")
         self.st.set_tiles(args.tiles)
-        self.lps = self.st.launches_per_step
         self.d = [torch.from_numpy(f).to(dev) for f in fields]
         self.st.load(self.d)
+        if args.launch == "auto" and args.tiles == -1:
+            self.st.autotune(10)  # launch form and tile shape, timed on this grid (state restored)
+        fused, tile = self.st.tiles()
+        self.launch = {"one_launch_per_time_step": fused, "tile_cfg": tile}
+        self.lps = self.st.launches_per_step
         self.st.set_graph(self.K)
         self.h_in = [torch.from_numpy(f).pin_memory() for f in fields]
         self.h_out = [torch.empty_like(h).pin_memory() for h in self.h_in]
@@ -325,7 +329,7 @@ def bench_ours(args):
             print(json.dumps({"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
                               "ms_per_step": ms_per_step, "roofline_achieved_gbs": achieved, "n": args.n,
                               "workload": workload, "dtype": args.dtype, "launches_per_time_step": run.lps,
-                              "note": "profiling run (--no-e2e)"}), flush=True)
+                              **getattr(run, "launch", {}), "note": "profiling run (--no-e2e)"}), flush=True)
         if world > 1:
             dist.barrier()
             dist.destroy_process_group()
@@ -385,6 +389,7 @@ def bench_ours(args):
             "data": data,
             "config": {"workload": workload, "shape": run.shape, "field_cells": run.cells,
                        "time_steps_per_step": K, "launches_per_time_step": run.lps,
+                       **getattr(run, "launch", {}),
                        "precision_note": "FP64 stencils" if run.prec == px.F64
                        else "FP32 stencils, compensated FP32 state, FP64 reductions",
                        "l2": "flushed between timed steps (256 MiB write); within a step the fields may stay "

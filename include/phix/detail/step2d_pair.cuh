@@ -1,0 +1,295 @@
+// step2d_pair.cuh -- one launch per RK4 step of 2-D Cahn-Hilliard on grids
+// whose four sides are periodic, with every thread advancing two x-adjacent
+// cells at a time.
+//
+// Same tile scheme as step2d.cuh (u on the tile + E loaded once, the four
+// stages in shared memory on regions shrinking by H per stage), arranged for
+// issue efficiency:
+//   * cells are processed as pairs: FP32 arithmetic uses the packed f32x2
+//     instructions of sm_100 (fma/add/mul .rn on both lanes, each lane
+//     rounded exactly as the scalar instruction), shared memory is read and
+//     written 8 (FP32) or 16 (FP64) bytes at a time;
+//   * each thread owns one pair column and a block of consecutive rows, so a
+//     5-point stencil keeps its north / centre / south pairs in registers and
+//     loads one pair plus the two side neighbours per row;
+//   * the k pass of stage s writes y_{s+1} = u + a k_s straight into the
+//     stage-state array (the CH k pass reads mu only) and folds k_s into the
+//     RK4 sum of the tile cells, so a stage is two passes and two barriers.
+// Regions are rounded outward to whole pairs; the extra cells read only
+// in-bounds shared memory and are never used by a cell that is kept.
+// Every cell sees the scalar path's operations in the scalar path's order
+// (Equation.cu:65-76 for the Laplacian, the CH driver's mu and rhs, the RK4
+// combination of Solver.cu), so the bits equal those of step_box / stage_box.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "step2d.cuh"
+
+namespace phix {
+
+// ---- pairs of cells -------------------------------------------------------
+template <typename T> struct PairOf;
+template <> struct PairOf<float> { using V = float2; };
+template <> struct PairOf<double> { using V = double2; };
+
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b rounded once: b * (-1) is exact, so fma(b, -1, a) = fl(a - b) on each lane
+__device__ __forceinline__ float2 p_sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 p_splat(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ double2 p_add(double2 a, double2 b) { return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y)); }
+__device__ __forceinline__ double2 p_mul(double2 a, double2 b) { return make_double2(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)); }
+__device__ __forceinline__ double2 p_fma(double2 a, double2 b, double2 c) {
+    return make_double2(__fma_rn(a.x, b.x, c.x), __fma_rn(a.y, b.y, c.y));
+}
+__device__ __forceinline__ double2 p_sub(double2 a, double2 b) { return make_double2(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y)); }
+__device__ __forceinline__ double2 p_splat(double v) { return make_double2(v, v); }
+
+template <typename T>
+__device__ __forceinline__ typename PairOf<T>::V p_ld(const T* p) {
+    return *reinterpret_cast<const typename PairOf<T>::V*>(p);
+}
+template <typename T>
+__device__ __forceinline__ void p_st(T* p, typename PairOf<T>::V v) {
+    *reinterpret_cast<typename PairOf<T>::V*>(p) = v;
+}
+
+// 5-point Laplacian of the pair c from its west, east, north (row - 1) and
+// south (row + 1) neighbour pairs (tile_lap: v2 = 2c; t = (f+ - v2) + f-;
+// v = tx*i2x; v = fma(ty, i2y, v)).  Returns v and leaves 2c in *v2.
+template <class V>
+__device__ __forceinline__ V p_lap(V c, V north, V south, V west, V east, V i2x, V i2y, V* v2) {
+    *v2 = p_add(c, c);  // 2*c: exact, equal to rmul(2, c)
+    const V tx = p_add(p_sub(east, *v2), west);
+    const V ty = p_add(p_sub(south, *v2), north);
+    return p_fma(ty, i2y, p_mul(tx, i2x));
+}
+
+template <typename T, int TX, int TY, int NRP>
+struct StepPair {
+    static constexpr int H = PolCH::H, E = 4 * H;
+    static constexpr int P = TX + 2 * E, R = TY + 2 * E;  // row pitch and rows of U, Y, M
+    static constexpr int NC = P / 2;                      // pair columns
+    static constexpr int NT = NC * NRP;                   // threads per CTA
+    static_assert(TX % 2 == 0 && E % 2 == 0, "pairs need an even tile width and halo");
+    static constexpr size_t smem_bytes() { return sizeof(T) * ((size_t)3 * P * R + (size_t)TX * TY); }
+};
+
+// A pass over the region e: rows [LO, LO + RH), cut into NRP blocks of B
+// consecutive rows (thread row phase rp takes rows LO + rp B ...), and the
+// pair columns [PLO, PHI), the region's columns rounded out to whole pairs.
+template <int TX, int TY, int E, int NRP, int e>
+struct PairRegion {
+    static constexpr int LO = E - e, RH = TY + 2 * e, B = (RH + NRP - 1) / NRP;
+    static constexpr int PLO = (E - e) >> 1, PHI = (E + TX + e + 1) >> 1;
+};
+
+// One mu pass: M = mu(Y) on the region e (rounded to pairs).
+template <typename T, int TX, int TY, int NRP, int e>
+__device__ __forceinline__ void pair_mu_pass(const StageArgs<T>& S, const T* __restrict__ Y, T* __restrict__ M,
+                                             int pc, int rp) {
+    using G = StepPair<T, TX, TY, NRP>;
+    using Rg = PairRegion<TX, TY, G::E, NRP, e>;
+    using V = typename PairOf<T>::V;
+    constexpr int P = G::P;
+    if (pc < Rg::PLO || pc >= Rg::PHI) return;
+    const int r0 = Rg::LO + rp * Rg::B;
+    const int nrows = min(Rg::B, Rg::LO + Rg::RH - r0);
+    if (nrows <= 0) return;
+    const T* y = Y + r0 * P + 2 * pc;
+    T* m = M + r0 * P + 2 * pc;
+    const V i2x = p_splat(S.i2[0]), i2y = p_splat(S.i2[1]);
+    const V two_rho = p_splat(S.p[2]), ca = p_splat(S.p[3]), cb = p_splat(S.p[4]);
+    const V mk = p_splat(S.p[1]), one = p_splat((T)1), zero = p_splat((T)0);
+    V n = p_ld(y - P), c = p_ld(y);
+#pragma unroll
+    for (int j = 0; j < Rg::B; ++j) {
+        if (j >= nrows) break;
+        const V s = p_ld(y + (j + 1) * P);
+        const T w = y[j * P - 1], ee = y[j * P + 2];
+        V v2;
+        const V lap = p_lap(c, n, s, V{w, c.x}, V{c.y, ee}, i2x, i2y, &v2);
+        // f'(c) = (two_rho (c - ca)) (c - cb) ((2c - ca) - cb)   (f_dw)
+        const V fa = p_mul(p_mul(two_rho, p_sub(c, ca)), p_sub(c, cb));
+        const V fd = p_mul(fa, p_sub(p_sub(v2, ca), cb));
+        // mu = (-kappa) lap + (1 f' + 0)   (PolCH::mu)
+        p_st(m + j * P, p_fma(mk, lap, p_fma(one, fd, zero)));
+        n = c;
+        c = s;
+    }
+}
+
+// One k pass (stages 1-3): k = M lap(mu) + 0 on the region e; Y = u + a k
+// there; the RK4 sum of the tile cells in ACC (k1, then + 2 k2, + 2 k3).
+template <typename T, int TX, int TY, int NRP, int e, int STAGE>
+__device__ __forceinline__ void pair_k_pass(const StageArgs<T>& S, const T* __restrict__ M, const T* __restrict__ U,
+                                            T* __restrict__ Y, T* __restrict__ ACC, T a, int pc, int rp) {
+    using G = StepPair<T, TX, TY, NRP>;
+    using Rg = PairRegion<TX, TY, G::E, NRP, e>;
+    using V = typename PairOf<T>::V;
+    constexpr int P = G::P, E = G::E;
+    if (pc < Rg::PLO || pc >= Rg::PHI) return;
+    const int r0 = Rg::LO + rp * Rg::B;
+    const int nrows = min(Rg::B, Rg::LO + Rg::RH - r0);
+    if (nrows <= 0) return;
+    const int off0 = r0 * P + 2 * pc;
+    const T* m = M + off0;
+    const V i2x = p_splat(S.i2[0]), i2y = p_splat(S.i2[1]);
+    const V mob = p_splat(S.p[0]), zero = p_splat((T)0), av = p_splat(a), two = p_splat((T)2);
+    const bool col_in = 2 * pc >= E && 2 * pc < E + TX;
+    V n = p_ld(m - P), c = p_ld(m);
+#pragma unroll
+    for (int j = 0; j < Rg::B; ++j) {
+        if (j >= nrows) break;
+        const V s = p_ld(m + (j + 1) * P);
+        const T w = m[j * P - 1], ee = m[j * P + 2];
+        V v2;
+        const V k = p_fma(mob, p_lap(c, n, s, V{w, c.x}, V{c.y, ee}, i2x, i2y, &v2), zero);
+        const int off = off0 + j * P;
+        p_st(Y + off, p_fma(av, k, p_ld(U + off)));
+        const int row = r0 + j;
+        if (col_in && row >= E && row < E + TY) {
+            T* acc = ACC + (row - E) * TX + 2 * pc - E;
+            p_st(acc, STAGE == 1 ? k : p_add(p_ld(acc), p_mul(two, k)));
+        }
+        n = c;
+        c = s;
+    }
+}
+
+template <typename T, int TX, int TY, int NRP>
+__device__ __forceinline__ void step_pair_tile(const StepArgs<T>& A, T* __restrict__ sm, int x0, int y0) {
+    using G = StepPair<T, TX, TY, NRP>;
+    using V = typename PairOf<T>::V;
+    constexpr int E = G::E, P = G::P, R = G::R, NC = G::NC;
+    T* U = sm;
+    T* Y = sm + P * R;
+    T* M = sm + 2 * P * R;
+    T* ACC = sm + 3 * P * R;
+    const StageArgs<T>& S = A.S;
+    const Layout& L = S.L;
+    const int n0 = L.n[0], n1 = L.n[1];
+    const int pc = threadIdx.x % NC, rp = threadIdx.x / NC;
+
+    // u on the tile + E (periodic images of out-of-domain cells): this
+    // thread's pair column on rows rp, rp + NRP, ...; all loads are issued
+    // before the first shared-memory store
+    const bool inside = x0 - E >= 0 && x0 + TX + E <= n0 && y0 - E >= 0 && y0 + TY + E <= n1;
+    {
+        constexpr int NLD = (R + NRP - 1) / NRP;
+        V v[NLD];
+        const int px = x0 - E + 2 * pc;
+#pragma unroll
+        for (int i = 0; i < NLD; ++i) {
+            const int ly = rp + i * NRP, py = y0 - E + ly;
+            if (ly < R) {
+                if (inside) {
+                    const T* g = S.u[0] + L.origin + px + L.s[1] * py;
+                    v[i] = V{__ldg(g), __ldg(g + 1)};
+                } else {
+                    int i0, i1;
+                    double cval;
+                    map3<2>(L, px, py, 0, &i0, &cval);  // periodic only: never MAP_CONST
+                    map3<2>(L, px + 1, py, 0, &i1, &cval);
+                    v[i] = V{__ldg(S.u[0] + i0), __ldg(S.u[0] + i1)};
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NLD; ++i) {
+            const int ly = rp + i * NRP;
+            if (ly < R) p_st(U + ly * P + 2 * pc, v[i]);
+        }
+    }
+    __syncthreads();
+
+    // stage 1: y1 = u
+    pair_mu_pass<T, TX, TY, NRP, 3 * G::H + 1>(S, U, M, pc, rp);
+    __syncthreads();
+    pair_k_pass<T, TX, TY, NRP, 3 * G::H, 1>(S, M, U, Y, ACC, A.dt2, pc, rp);
+    __syncthreads();
+    // stage 2
+    pair_mu_pass<T, TX, TY, NRP, 2 * G::H + 1>(S, Y, M, pc, rp);
+    __syncthreads();
+    pair_k_pass<T, TX, TY, NRP, 2 * G::H, 2>(S, M, U, Y, ACC, A.dt2, pc, rp);
+    __syncthreads();
+    // stage 3
+    pair_mu_pass<T, TX, TY, NRP, G::H + 1>(S, Y, M, pc, rp);
+    __syncthreads();
+    pair_k_pass<T, TX, TY, NRP, G::H, 3>(S, M, U, Y, ACC, A.dt, pc, rp);
+    __syncthreads();
+    // stage 4
+    pair_mu_pass<T, TX, TY, NRP, 1>(S, Y, M, pc, rp);
+    __syncthreads();
+
+    // k4 on the tile, then u' = u + dt/6 (((k1 + 2 k2) + 2 k3) + k4)
+    {
+        using Rg = PairRegion<TX, TY, E, NRP, 0>;
+        const int r0 = Rg::LO + rp * Rg::B;
+        const int nrows = min(Rg::B, Rg::LO + Rg::RH - r0);
+        if (pc >= Rg::PLO && pc < Rg::PHI && nrows > 0) {
+            const int off0 = r0 * P + 2 * pc;
+            const T* m = M + off0;
+            const V i2x = p_splat(S.i2[0]), i2y = p_splat(S.i2[1]);
+            const V mob = p_splat(S.p[0]), zero = p_splat((T)0), dtf = p_splat(S.dtf);
+            const int gx = x0 + 2 * pc - E;  // x of the pair's first cell
+            const bool x1 = gx + 1 < n0;
+            V n = p_ld(m - P), c = p_ld(m);
+#pragma unroll
+            for (int j = 0; j < Rg::B; ++j) {
+                if (j >= nrows) break;
+                const V s = p_ld(m + (j + 1) * P);
+                const T w = m[j * P - 1], ee = m[j * P + 2];
+                V v2;
+                const V k = p_fma(mob, p_lap(c, n, s, V{w, c.x}, V{c.y, ee}, i2x, i2y, &v2), zero);
+                n = c;
+                c = s;
+                const int row = r0 + j, py = y0 + row - E;
+                if (py >= n1 || gx >= n0) break;  // past the grid (partial tiles)
+                const V sum = p_add(p_ld(ACC + (row - E) * TX + 2 * pc - E), k);
+                const V u = p_ld(U + off0 + j * P);
+                const V d = p_mul(dtf, sum);
+                const int idx = L.origin + gx + L.s[1] * py;
+                if (S.ulo[0]) {
+                    twosum_update(u.x, __ldg(S.ulo[0] + idx), d.x, &S.out[0][idx], &S.outlo[0][idx]);
+                    if (x1) twosum_update(u.y, __ldg(S.ulo[0] + idx + 1), d.y, &S.out[0][idx + 1],
+                                          &S.outlo[0][idx + 1]);
+                } else {
+                    const V o = p_fma(dtf, sum, u);
+                    S.out[0][idx] = o.x;
+                    if (x1) S.out[0][idx + 1] = o.y;
+                }
+            }
+        }
+    }
+    if (!inside) box_ghosts<T, 2, 1, TX, TY, G::NT>(S, x0, y0);
+}
+
+template <typename T, int TX, int TY, int NRP>
+__global__ void __launch_bounds__(StepPair<T, TX, TY, NRP>::NT) step_pair(const StepArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char step_smem[];
+    step_pair_tile<T, TX, TY, NRP>(A, reinterpret_cast<T*>(step_smem), blockIdx.x * TX, blockIdx.y * TY);
+}
+
+// Many fields in one launch: one CTA per entry of the tile list.
+template <typename T, int TX, int TY, int NRP>
+__global__ void __launch_bounds__(StepPair<T, TX, TY, NRP>::NT)
+    step_pair_batched(const StepArgs<T>* __restrict__ args, const BatchTile* __restrict__ tiles) {
+    extern __shared__ __align__(16) unsigned char step_smem[];
+    const BatchTile bt = tiles[blockIdx.x];
+    const StepArgs<T> a = args[bt.inst];
+    step_pair_tile<T, TX, TY, NRP>(a, reinterpret_cast<T*>(step_smem), bt.x0, bt.y0);
+}
+
+// Grids the pair kernels take: 2-D, four periodic sides.
+inline bool step_pair_supported(const Layout& L, int dim) {
+    if (dim != 2) return false;
+    for (int i = 0; i < 4; ++i)
+        if (L.bc[i] != PHIX_BC_PERIODIC) return false;
+    return true;
+}
+
+}  // namespace phix

@@ -158,9 +158,10 @@ int phix_stepper_set_graph(phix_stepper_t* h, int steps_per_graph);
 
 /* 1: where supported, run each RK4 step as one launch that keeps the four
  * stage states in shared memory and recomputes the tile halos; 0: one launch
- * per stage.  Both give the same bits.  Default: 1 for FP32 steppers, 0 for
- * FP64 (the faster of the two on B200 for each).  No reference counterpart
- * (the reference runs each term and stage as its own kernels). */
+ * per stage.  Both give the same bits.  Default: 1 for FP32 steppers and for
+ * FP64 CH steppers whose four sides are periodic (the pair kernels), else 0
+ * (the faster of the two on B200 for each).  No reference counterpart (the
+ * reference runs each term and stage as its own kernels). */
 int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step);
 
 /* Kernel launches one time step takes with the current settings. */
@@ -169,11 +170,24 @@ int phix_stepper_launches_per_step(const phix_stepper_t* h);
 /* Tile shape of the 2-D kernels.  One launch per stage: -1 the box tiles
  * (64x16, 256 threads, flat cell loops), 0..3 column-walking tiles (TX x TY =
  * 64x16, 64x32, 128x16, 32x16 with 4, 4, 2, 8 row groups; 256 threads).  One
- * launch per RK4 step: 0..5 tiles of 64x16, 64x32, 128x16, 128x32 (512
- * threads), 128x64 and 256x32 (1024 threads; FP32 only, where they fit in
- * shared memory); -1 picks 128x64 for FP32 grids of at most one wave of such
- * tiles, else 128x32.  All give the same bits.  No reference counterpart. */
+ * launch per RK4 step: 0..5 cell-per-thread tiles of 64x16, 64x32, 128x16,
+ * 128x32 (512 threads), 128x64 and 256x32 (1024 threads; FP32 only);
+ * 6..15 pair tiles (CH with four periodic sides; two cells per thread) of
+ * 128x64, 128x32, 128x32, 128x16, 64x32, 64x64, 256x32, 128x28, 64x28, 64x16
+ * with 8, 8, 4, 4, 8, 8, 4, 8, 8, 4 row blocks.  Shapes that do not fit in
+ * shared memory for the precision are refused when the step runs.  -1 picks
+ * by grid (see phix_stepper_autotune for a measured choice).  All give the
+ * same bits.  No reference counterpart. */
 int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg);
+
+/* The current launch form (1: one launch per RK4 step) and tile shape. */
+int phix_stepper_get_tiles(const phix_stepper_t* h, int* one_launch_per_step, int* tile_cfg);
+
+/* Time every launch form (one launch per stage or per RK4 step) and tile
+ * shape this stepper's grid can take, twice on trial_steps steps of its
+ * current state, keep the fastest (state saved and restored); *best_ms = ms
+ * per step.  RK4 and Euler steppers.  No reference counterpart. */
+int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms);
 
 /* FP64 only: run directly on caller-owned buffers, no copies.  fields[f] is
  * the current state and alt[f] a second stored array of the same size.
@@ -202,8 +216,10 @@ int phix_batch_create(phix_batch_t** out, int phys, int scheme, int precision, i
                       const double* prm, double dt);
 int phix_batch_destroy(phix_batch_t* b);
 
-/* 1: run each RK4 step of the whole batch as one launch (one CTA per 128x32
- * tile, the four stage states in shared memory, tile halos recomputed);
+/* 1: run each RK4 step of the whole batch as one launch (one CTA per tile,
+ * the four stage states in shared memory, tile halos recomputed; the pair
+ * kernels with 128x32 (FP32) or 64x32 (FP64) tiles when every instance is
+ * CH with four periodic sides, else 128x32 cell-per-thread tiles);
  * needs RK4 and periodic or zero-flux sides on every instance, else
  * PHIX_ERR_UNSUPPORTED.  0: one launch per stage.  Both give the same bits.
  * Default: 1 wherever it is possible (the faster on B200 in both

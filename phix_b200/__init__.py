@@ -107,6 +107,8 @@ def lib() -> C.CDLL:
         "phix_stepper_set_fusion": ([vp, C.c_int], C.c_int),
         "phix_stepper_launches_per_step": ([vp], C.c_int),
         "phix_stepper_set_tiles": ([vp, C.c_int], C.c_int),
+        "phix_stepper_autotune": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
+        "phix_stepper_get_tiles": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
         "phix_stepper_bind": ([vp, C.POINTER(vp), C.POINTER(vp)], C.c_int),
         "phix_stepper_current": ([vp], C.c_int),
         "phix_stepper_run_host": ([vp, C.POINTER(vp), C.POINTER(vp), C.c_int], C.c_int),
@@ -278,8 +280,22 @@ class Stepper:
         return lib().phix_stepper_launches_per_step(self.h)
 
     def set_tiles(self, cfg: int):
-        """2-D stage tile shape (0..3 column-walking tiles, -1 generic box tiles)."""
+        """2-D tile shape: one launch per stage -1 (box) or 0..3 (column
+        tiles); one launch per RK4 step 0..15 (6..15 pair tiles), -1 by grid."""
         check(lib().phix_stepper_set_tiles(self.h, cfg))
+
+    def tiles(self):
+        """(one launch per RK4 step?, tile configuration) currently in use."""
+        f, t = C.c_int(), C.c_int()
+        check(lib().phix_stepper_get_tiles(self.h, C.byref(f), C.byref(t)))
+        return bool(f.value), t.value
+
+    def autotune(self, trial_steps: int = 3) -> float:
+        """Time every launch form and tile shape on the current state (which
+        is restored), keep the fastest; returns its ms per step."""
+        ms = C.c_double()
+        check(lib().phix_stepper_autotune(self.h, trial_steps, C.byref(ms)))
+        return ms.value
 
     def bind(self, fields, alt):
         check(lib().phix_stepper_bind(self.h, _ptrs(fields), _ptrs(alt)))

@@ -17,6 +17,7 @@
 #include "phix/detail/common.cuh"
 #include "phix/detail/stage.cuh"
 #include "phix/detail/step2d.cuh"
+#include "phix/detail/step2d_pair.cuh"
 #include "stepper.h"
 
 namespace phix {
@@ -75,6 +76,29 @@ int batched_step(int phys, bool prepare, const StepArgs<T>* args, const BatchTil
                  cudaStream_t s) {
     if (phys == PHIX_PHYS_AC) return batched_step_cfg<T, PHIX_PHYS_AC>(prepare, args, tiles, ntiles, nsm, s);
     return batched_step_cfg<T, PHIX_PHYS_CH>(prepare, args, tiles, ntiles, nsm, s);
+}
+
+// The pair kernels (step2d_pair.cuh) where every instance is CH with four
+// periodic sides: tiles of 128x32 (FP32) or 64x32 (FP64), 8 row blocks; 32
+// rows divide every grid size of the batched CH workload.
+template <typename T> struct BatchPair;
+template <> struct BatchPair<float> { static constexpr int TX = 128, TY = 32, NRP = 8; };
+template <> struct BatchPair<double> { static constexpr int TX = 64, TY = 32, NRP = 8; };
+
+template <typename T>
+int batched_pair(bool prepare, const StepArgs<T>* args, const BatchTile* tiles, int ntiles, cudaStream_t s) {
+    using C = BatchPair<T>;
+    using G = StepPair<T, C::TX, C::TY, C::NRP>;
+    static_assert(G::smem_bytes() <= 227 * 1024, "batched pair tile exceeds shared memory");
+    auto kern = step_pair_batched<T, C::TX, C::TY, C::NRP>;
+    if (prepare) {
+        PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
+        return PHIX_OK;
+    }
+    if (ntiles < 1) return PHIX_OK;
+    kern<<<ntiles, G::NT, G::smem_bytes(), s>>>(args, tiles);
+    PHIX_LAUNCH_CHECK("step_pair_batched");
+    return PHIX_OK;
 }
 
 template <typename T, int PHYS, int MODE>
@@ -183,6 +207,7 @@ struct phix_batch {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     // one launch per RK4 step (possible where every side is periodic or zero-flux)
     bool can_fuse = false, fuse_steps = false;
+    bool step_pair = false;  // the fused step runs the pair kernels
     void* step_args_dev = nullptr;  // [parity][ninst] StepArgs
     BatchTile* step_tiles_dev = nullptr;
     int step_ntiles = 0;
@@ -324,13 +349,17 @@ int build_step(phix_batch* b) {
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
         return (long long)b->grids[a].n[0] * b->grids[a].n[1] > (long long)b->grids[c].n[0] * b->grids[c].n[1];
     });
+    b->step_pair = b->phys == PHIX_PHYS_CH;
+    for (int i = 0; i < b->ninst && b->step_pair; ++i) b->step_pair = step_pair_supported(b->layouts[i], 2);
+    const int tx = b->step_pair ? BatchPair<T>::TX : BST_TX, ty = b->step_pair ? BatchPair<T>::TY : BST_TY;
     std::vector<BatchTile> tiles;
     for (int i : order)
-        for (int y = 0; y < b->grids[i].n[1]; y += BST_TY)
-            for (int x = 0; x < b->grids[i].n[0]; x += BST_TX) tiles.push_back({i, x, y, 0});
+        for (int y = 0; y < b->grids[i].n[1]; y += ty)
+            for (int x = 0; x < b->grids[i].n[0]; x += tx) tiles.push_back({i, x, y, 0});
     b->step_ntiles = (int)tiles.size();
     PHIX_TRY_CUDA(cudaMalloc(&b->step_tiles_dev, sizeof(BatchTile) * tiles.size()));
     PHIX_TRY_CUDA(cudaMemcpy(b->step_tiles_dev, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice));
+    if (b->step_pair) return batched_pair<T>(true, nullptr, nullptr, 0, nullptr);
     return batched_step<T>(b->phys, true, nullptr, nullptr, 0, 0, nullptr);
 }
 
@@ -340,7 +369,9 @@ int batch_step(phix_batch* b, cudaStream_t s) {
     int rc;
     if (b->fuse_steps) {
         const StepArgs<T>* args = reinterpret_cast<const StepArgs<T>*>(b->step_args_dev) + (size_t)par * b->ninst;
-        if ((rc = batched_step<T>(b->phys, false, args, b->step_tiles_dev, b->step_ntiles, b->nsm, s))) return rc;
+        rc = b->step_pair ? batched_pair<T>(false, args, b->step_tiles_dev, b->step_ntiles, s)
+                          : batched_step<T>(b->phys, false, args, b->step_tiles_dev, b->step_ntiles, b->nsm, s);
+        if (rc) return rc;
     } else if (b->scheme == PHIX_EULER) {
         rc = launch_batched<T>(b->phys, MODE_EULER_FINAL, b->cfg, args_table<T>(b, 4, par), b->tiles_dev, b->ntiles,
                                b->ctas_per_sm, b->nsm, s);

@@ -9,15 +9,19 @@
 // Euler step = 1 launch: u' = u + dt F(u).
 // The state ping-pongs between two buffers; k buffers are per field.  Groups
 // of steps can be captured once into a CUDA graph and replayed.
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <algorithm>
+#include <utility>
 #include <vector>
 
 #include "phix/detail/common.cuh"
 #include "phix/detail/stage.cuh"
 #include "phix/detail/stage_col.cuh"
 #include "phix/detail/step2d.cuh"
+#include "phix/detail/step2d_pair.cuh"
 #include "stepper.h"
 
 namespace phix {
@@ -160,6 +164,11 @@ constexpr int kStepCfgs[][3] = {{64, 16, 256}, {64, 32, 256}, {128, 16, 256}, {1
                                  {256, 32, 1024}};
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100
 constexpr int kNumStepCfgs = sizeof(kStepCfgs) / sizeof(kStepCfgs[0]);
+// tiles of the pair kernels (CH, four periodic sides): (TX, TY, row blocks);
+// threads = (TX / 2 + 8) x row blocks.  Step configuration kNumStepCfgs + i.
+constexpr int kPairCfgs[][3] = {{128, 64, 8}, {128, 32, 8}, {128, 32, 4}, {128, 16, 4}, {64, 32, 8},
+                                 {64, 64, 8},  {256, 32, 4}, {128, 28, 8}, {64, 28, 8},  {64, 16, 4}};
+constexpr int kNumPairCfgs = sizeof(kPairCfgs) / sizeof(kPairCfgs[0]);
 
 template <typename T, class Pol, int TX, int TY, int NT>
 int step_cfg(bool prepare, const StepArgs<T>* A, cudaStream_t s) {
@@ -198,12 +207,65 @@ int step_dispatch(int cfg, bool prepare, const StepArgs<T>* A, cudaStream_t s) {
     return PHIX_ERR_ARG;
 }
 
+// prepare: set the shared-memory attribute; occ != nullptr: report resident
+// CTAs per SM (0: does not fit); else launch.
+template <typename T, int TX, int TY, int NRP>
+int pair_cfg(bool prepare, const StepArgs<T>* A, cudaStream_t s, int* occ = nullptr) {
+    using G = StepPair<T, TX, TY, NRP>;
+    if (G::smem_bytes() > kMaxSmem) {
+        if (occ) *occ = 0;
+        if (prepare || occ) return PHIX_OK;
+        set_error("step_pair: a %dx%d tile needs %zu bytes of shared memory", TX, TY, G::smem_bytes());
+        return PHIX_ERR_UNSUPPORTED;
+    }
+    if (occ) {
+        PHIX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, step_pair<T, TX, TY, NRP>, G::NT,
+                                                                    G::smem_bytes()));
+        return PHIX_OK;
+    }
+    if (prepare) {
+        PHIX_TRY_CUDA(cudaFuncSetAttribute(step_pair<T, TX, TY, NRP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)G::smem_bytes()));
+        return PHIX_OK;
+    }
+    dim3 grid((A->S.L.n[0] + TX - 1) / TX, (A->S.L.n[1] + TY - 1) / TY, 1);
+    step_pair<T, TX, TY, NRP><<<grid, G::NT, G::smem_bytes(), s>>>(*A);
+    PHIX_LAUNCH_CHECK("step_pair");
+    return PHIX_OK;
+}
+
+template <typename T>
+int pair_dispatch(int i, bool prepare, const StepArgs<T>* A, cudaStream_t s, int* occ = nullptr) {
+    switch (i) {
+#define PHIX_PAIR_CASE(i) \
+    case i: return pair_cfg<T, kPairCfgs[i][0], kPairCfgs[i][1], kPairCfgs[i][2]>(prepare, A, s, occ);
+        PHIX_PAIR_CASE(0)
+        PHIX_PAIR_CASE(1)
+        PHIX_PAIR_CASE(2)
+        PHIX_PAIR_CASE(3)
+        PHIX_PAIR_CASE(4)
+        PHIX_PAIR_CASE(5)
+        PHIX_PAIR_CASE(6)
+        PHIX_PAIR_CASE(7)
+        PHIX_PAIR_CASE(8)
+        PHIX_PAIR_CASE(9)
+#undef PHIX_PAIR_CASE
+    }
+    set_error("step_pair: bad tile configuration %d", i);
+    return PHIX_ERR_ARG;
+}
+
 template <typename T, int PHYS>
 int prepare_step2d_t() {
     for (int c = 0; c < kNumStepCfgs; ++c) {
         int rc = step_dispatch<T, PHYS>(c, true, nullptr, 0);
         if (rc) return rc;
     }
+    if (PHYS == PHIX_PHYS_CH)
+        for (int c = 0; c < kNumPairCfgs; ++c) {
+            int rc = pair_dispatch<T>(c, true, nullptr, 0);
+            if (rc) return rc;
+        }
     return PHIX_OK;
 }
 
@@ -245,17 +307,44 @@ int prepare_stage(int phys, int dim, int prec) {
     return prec == PHIX_F32 ? prepare_t<float>(phys) : prepare_t<double>(phys);
 }
 
+// Pair tile for a grid: among the shapes with at least two resident CTAs
+// and 1024 (FP32) or 512 (FP64) resident threads per SM (fewer leave too few
+// warps to hide the barriers' latency), the least (waves x CTAs per SM x
+// work per tile), work per tile being the cells of the eight passes'
+// regions; ties go to the earlier shape.  On B200 this picks 128x28 (FP32)
+// and 64x28 (FP64) at 1024^2 and 128x32 for FP32 at 4096^2, the fastest
+// measured there.
+template <typename T>
+int pick_pair_cfg(const Layout& L, int nsm) {
+    int best = 1;
+    double best_cost = 1e300;
+    for (int i = 0; i < kNumPairCfgs; ++i) {
+        int occ = 0;
+        if (pair_dispatch<T>(i, false, nullptr, 0, &occ) != PHIX_OK || occ < 2) continue;
+        const int tx = kPairCfgs[i][0], ty = kPairCfgs[i][1];
+        if (occ * (tx / 2 + 8) * kPairCfgs[i][2] < (sizeof(T) == 4 ? 1024 : 512)) continue;
+        const double tiles = (double)((L.n[0] + tx - 1) / tx) * ((L.n[1] + ty - 1) / ty);
+        const double waves = std::ceil(tiles / ((double)nsm * occ));
+        double work = 0.0;
+        for (int e = 0; e <= 7; ++e) work += (double)(tx + 2 * e + (e & 1)) * (ty + 2 * e);
+        const double cost = waves * occ * work;
+        if (cost < best_cost) { best_cost = cost; best = i; }
+    }
+    return best;
+}
+
 // Default tile of the one-launch step (measured on B200): 128x32 with 512
 // threads, or 128x64 with 1024 threads in FP32 when those tiles fill at most
 // one wave (one CTA per SM: the smaller grids, e.g. 1024^2).
 template <typename T>
-int default_step_cfg(const Layout& L) {
+int default_step_cfg(int phys, const Layout& L) {
     static int nsm = 0;
     if (!nsm) {
         int dev = 0;
         cudaGetDevice(&dev);
         if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
     }
+    if (phys == PHIX_PHYS_CH && step_pair_supported(L, 2)) return kNumStepCfgs + pick_pair_cfg<T>(L, nsm);
     if (sizeof(T) == 4) {
         const long long tiles = (long long)((L.n[0] + 127) / 128) * ((L.n[1] + 63) / 64);
         if (tiles <= nsm) return 4;
@@ -265,7 +354,14 @@ int default_step_cfg(const Layout& L) {
 
 template <typename T>
 int launch_step2d(int phys, const StepArgs<T>& A, cudaStream_t s, int tile) {
-    const int cfg = tile < 0 ? default_step_cfg<T>(A.S.L) : tile;
+    const int cfg = tile < 0 ? default_step_cfg<T>(phys, A.S.L) : tile;
+    if (cfg >= kNumStepCfgs) {
+        if (phys != PHIX_PHYS_CH || !step_pair_supported(A.S.L, 2)) {
+            set_error("step_pair: tile configuration %d needs CH with four periodic sides", cfg);
+            return PHIX_ERR_UNSUPPORTED;
+        }
+        return pair_dispatch<T>(cfg - kNumStepCfgs, false, &A, s);
+    }
     if (phys == PHIX_PHYS_AC) return step_dispatch<T, PHIX_PHYS_AC>(cfg, false, &A, s);
     if (phys == PHIX_PHYS_CH) return step_dispatch<T, PHIX_PHYS_CH>(cfg, false, &A, s);
     set_error("step2d: physics %d has more than one field", phys);
@@ -546,9 +642,10 @@ int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precisio
     h->L = L;
     h->S = S;
     h->esz = precision == PHIX_F32 ? 4 : 8;
-    // measured on B200 at 1024^2: the one-launch step wins in FP32 and loses in
-    // FP64 (twice the shared memory per tile, half the resident tiles)
-    h->fuse_steps = precision == PHIX_F32;
+    // measured on B200 at 1024^2: the one-launch step wins in FP32, and in FP64
+    // where the pair kernel takes the grid (CH, four periodic sides); the
+    // cell-per-thread step kernel loses to one launch per stage in FP64
+    h->fuse_steps = precision == PHIX_F32 || (phys == PHIX_PHYS_CH && step_pair_supported(L, g->dim));
     auto fail = [&](cudaError_t e, const char* w) {
         int r = cuda_status(e, w);
         phix_stepper_destroy(h);
@@ -630,7 +727,8 @@ int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step) {
 int phix_stepper_launches_per_step(const phix_stepper_t* h) { return h ? launches_per_step(h) : -1; }
 
 int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg) {
-    if (!h || tile_cfg < -1 || tile_cfg >= (kNumColCfgs > kNumStepCfgs ? kNumColCfgs : kNumStepCfgs)) {
+    if (!h || tile_cfg < -1 || tile_cfg >= (kNumColCfgs > kNumStepCfgs + kNumPairCfgs ? kNumColCfgs
+                                                                                       : kNumStepCfgs + kNumPairCfgs)) {
         set_error("set_tiles: bad stepper or configuration");
         return PHIX_ERR_ARG;
     }
@@ -638,6 +736,93 @@ int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg) {
         drop_graphs(h);
         h->tile = tile_cfg;
     }
+    return PHIX_OK;
+}
+
+int phix_stepper_get_tiles(const phix_stepper_t* h, int* one_launch_per_step, int* tile_cfg) {
+    if (!h) { set_error("get_tiles: NULL stepper"); return PHIX_ERR_ARG; }
+    if (one_launch_per_step) *one_launch_per_step = step_fused(h) ? 1 : 0;
+    if (tile_cfg) *tile_cfg = h->tile;
+    return PHIX_OK;
+}
+
+int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms) {
+    if (!h || trial_steps < 1) { set_error("autotune: bad stepper or trial_steps"); return PHIX_ERR_ARG; }
+    if (h->scheme == PHIX_MULTISTEP) {
+        set_error("autotune: RK4 and Euler steppers only");
+        return PHIX_ERR_UNSUPPORTED;
+    }
+    // candidates: one launch per stage with every stage tile, and (RK4, one
+    // 2-D field with periodic or zero-flux sides) one launch per step with
+    // every step tile
+    std::vector<std::pair<bool, int>> cand;
+    if (h->dim == 2)
+        for (int t = -1; t < kNumColCfgs; ++t) cand.push_back({false, t});
+    else
+        cand.push_back({false, -1});
+    if (h->scheme == PHIX_RK4 && h->nf == 1 && step2d_supported(h->L, h->dim))
+        for (int t = 0; t < kNumStepCfgs + kNumPairCfgs; ++t) cand.push_back({true, t});
+
+    // trials advance the state: save it, and restore it afterwards
+    const int cur0 = h->cur;
+    const bool bc0 = h->bc_pending, fuse0 = h->fuse_steps;
+    const int tile0 = h->tile, graph0 = h->graph_steps;
+    const size_t bytes = h->S * h->esz;
+    const int parts = h->lo[cur0][0] ? 2 : 1;
+    void* save = nullptr;
+    PHIX_TRY_CUDA(cudaMalloc(&save, bytes * h->nf * parts));
+    auto copy_state = [&](bool to_save) {
+        for (int f = 0; f < h->nf; ++f)
+            for (int q = 0; q < parts; ++q) {
+                void* buf = q ? h->lo[cur0][f] : h->st[cur0][f];
+                char* sv = (char*)save + bytes * (f * parts + q);
+                cudaError_t e = to_save ? cudaMemcpy(sv, buf, bytes, cudaMemcpyDeviceToDevice)
+                                        : cudaMemcpy(buf, sv, bytes, cudaMemcpyDeviceToDevice);
+                if (e != cudaSuccess) return cuda_status(e, "autotune: state copy");
+            }
+        return (int)PHIX_OK;
+    };
+    int rc = copy_state(true);
+    drop_graphs(h);
+    h->graph_steps = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = cuda_status(cudaGetLastError(), "autotune: cudaEventCreate");
+    float best = 1e30f;
+    bool best_fuse = fuse0;
+    int best_tile = tile0;
+    for (size_t c = 0; c < cand.size() && !rc; ++c) {
+        h->fuse_steps = cand[c].first;
+        h->tile = cand[c].second;
+        int r = enqueue_steps(h, 1, 0);  // warm-up; shapes this grid cannot take are skipped
+        if (r == PHIX_ERR_UNSUPPORTED) continue;
+        if (r) { rc = r; break; }
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2 && !rc; ++rep) {  // the faster of two timings
+            cudaEventRecord(e0, 0);
+            if ((rc = enqueue_steps(h, trial_steps, 0))) break;
+            cudaEventRecord(e1, 0);
+            cudaError_t e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) { rc = cuda_status(e, "autotune: trial"); break; }
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms = std::min(ms, t);
+        }
+        if (rc) break;
+        if (ms < best) { best = ms; best_fuse = cand[c].first; best_tile = cand[c].second; }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    h->cur = cur0;
+    const int rc2 = copy_state(false);
+    cudaFree(save);
+    h->bc_pending = bc0;
+    h->graph_steps = graph0;
+    h->fuse_steps = rc ? fuse0 : best_fuse;
+    h->tile = rc ? tile0 : best_tile;
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (best_ms) *best_ms = best / trial_steps;
     return PHIX_OK;
 }
 

@@ -83,10 +83,14 @@ def test_batch_mass_and_autotune(cuda):
 
 @pytest.mark.parametrize("prec", [px.F64, px.F32])
 @pytest.mark.parametrize("graph", [0, 3])
-def test_batch_one_launch_step_matches_single_field_stepper(cuda, prec, graph):
+@pytest.mark.parametrize("all_periodic", [False, True])
+def test_batch_one_launch_step_matches_single_field_stepper(cuda, prec, graph, all_periodic):
     """One launch per RK4 step over the whole batch gives each instance the
-    bits of the single-field stepper."""
+    bits of the single-field stepper (the pair kernels when every instance
+    is periodic, the cell-per-thread kernel with a zero-flux instance)."""
     grids, phys, prms, scheme, dt, fields = small_batch(prec)
+    if all_periodic:
+        grids[1] = px.make_grid((40, 40))
     b = px.Batch(phys, scheme, prec, grids, prms, dt)
     assert b.launches_per_step == 1  # the default where every side allows it
     b.set_fusion(False)

@@ -173,7 +173,13 @@ FUSED_CASES = [
     (px.PHYS_CH, (9, 30), px.BC_NOFLUX, px.BC_NOFLUX, (1.0, 1.0)),
     (px.PHYS_AC, (200, 33), px.BC_PERIODIC, px.BC_PERIODIC, (1.0, 0.7)),
     (px.PHYS_AC, (66, 65), px.BC_NOFLUX, px.BC_NOFLUX, (1.0, 1.0)),
+    (px.PHYS_CH, (300, 170), px.BC_PERIODIC, px.BC_PERIODIC, (1.0, 0.8)),
 ]
+
+# one-launch step tiles: 0-5 the box kernel, 6-15 the pair kernel (CH with
+# four periodic sides); those that do not fit in shared memory per precision
+STEP_TILES = {px.F64: (0, 1, 2, 3, 7, 8, 9, 10, 11, 13, 14, 15), px.F32: tuple(range(16))}
+PAIR_TILES = set(range(6, 16))
 
 
 @pytest.mark.parametrize("prec", [px.F64, px.F32])
@@ -312,9 +318,10 @@ def test_stage_tile_shapes_give_identical_bits(cuda, oracle, prec, case):
 
 
 @pytest.mark.parametrize("prec", [px.F64, px.F32])
-@pytest.mark.parametrize("case", [0, 1, 5])
+@pytest.mark.parametrize("case", [0, 1, 5, 6])
 def test_one_launch_step_tile_shapes(cuda, prec, case):
-    """Every tile shape of the one-launch RK4 step gives the per-stage bits."""
+    """Every tile shape of the one-launch RK4 step gives the per-stage bits
+    (the pair kernels on the CH grids with four periodic sides)."""
     phys, n, bx, by, d = FUSED_CASES[case]
     bcs = (bx, bx, by, by, 0, 0)
     g = px.make_grid(n, d, 1, bcs)
@@ -325,9 +332,9 @@ def test_one_launch_step_tile_shapes(cuda, prec, case):
     prm = [1.0, 0.6, 1.2, 0.05, 0.95] if phys == px.PHYS_CH else [0.8, 1.3]
     dt = 0.004 if phys == px.PHYS_CH else 0.02
     outs = {}
-    tiles = ((False, -1), (True, -1), (True, 0), (True, 1), (True, 2), (True, 3))
-    if prec == px.F32:
-        tiles += ((True, 4), (True, 5))
+    pair_ok = phys == px.PHYS_CH and bx == by == px.BC_PERIODIC
+    tiles = ((False, -1), (True, -1)) + tuple(
+        (True, t) for t in STEP_TILES[prec] if pair_ok or t not in PAIR_TILES)
     for fused, tile in tiles:
         st = px.Stepper(phys, px.RK4, prec, prm, dt, g)
         st.set_fusion(fused)
@@ -343,3 +350,49 @@ def test_one_launch_step_tile_shapes(cuda, prec, case):
     base = outs[(False, -1)]
     for key, a in outs.items():
         assert np.array_equal(a[keep], base[keep]), (key, _where(a, base, keep))
+
+
+def test_pair_step_tiles_need_periodic_ch(cuda):
+    g = px.make_grid((64, 40), bc=(px.BC_NOFLUX,) * 2 + (px.BC_PERIODIC,) * 4)
+    st = px.Stepper(px.PHYS_CH, px.RK4, px.F32, [1.0, 0.6, 1.2, 0.05, 0.95], 0.004, g)
+    st.set_fusion(True)
+    st.set_tiles(7)
+    t = torch.full(px.stored_shape(g), 0.5, dtype=torch.float64, device="cuda")
+    st.load([t])
+    with pytest.raises(px.PhixError):
+        st.advance(1)
+    st.close()
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32])
+def test_autotune_restores_state_and_keeps_bits(cuda, prec):
+    """Autotuning leaves the loaded state as it was, and the launch form and
+    tile it keeps give the per-stage bits."""
+    phys, n, bx, by, d = FUSED_CASES[6]
+    bcs = (bx, bx, by, by, 0, 0)
+    g = px.make_grid(n, d, 1, bcs)
+    grid = Grid(n=n, d=d, bc=bcs, bc_val=(0,) * 6)
+    x = grid.stored_from_phys(np.random.default_rng(77).uniform(0.3, 0.7, size=(1, n[1], n[0])))
+    prm, dt = [1.0, 0.6, 1.2, 0.05, 0.95], 0.004
+    outs, loaded = [], []
+    for tune in (False, True):
+        st = px.Stepper(phys, px.RK4, prec, prm, dt, g)
+        t = torch.from_numpy(x.copy()).cuda()
+        st.load([t])
+        if tune:
+            assert st.autotune(2) > 0
+            fused, tile = st.tiles()
+            assert st.launches_per_step == (1 if fused else 4)
+        else:
+            st.set_fusion(False)
+        back = torch.empty_like(t)
+        st.store([back])  # FP32: the compensated pair of x, as loaded
+        st.advance(6)
+        st.store([t])
+        torch.cuda.synchronize()
+        st.close()
+        loaded.append(back.cpu().numpy())
+        outs.append(t.cpu().numpy())
+    keep = ~corner_mask(grid)
+    assert np.array_equal(loaded[0][keep], loaded[1][keep])
+    assert np.array_equal(outs[0][keep], outs[1][keep]), _where(outs[1], outs[0], keep)
