@@ -76,16 +76,48 @@ struct StepPair {
     static constexpr int NT = NC * NRP;                   // threads per CTA
     static_assert(TX % 2 == 0 && E % 2 == 0, "pairs need an even tile width and halo");
     static constexpr size_t smem_bytes() { return sizeof(T) * ((size_t)3 * P * R + (size_t)TX * TY); }
+    // CTAs per SM that the shared memory admits (228 KB per SM, 1 KB reserved
+    // per CTA), at most 2048 threads: the launch bound asks ptxas to keep
+    // the registers within that many CTAs
+    static constexpr int FIT = (int)((228 * 1024) / (smem_bytes() + 1024));
+    static constexpr int MINB = FIT < 1 ? 1 : (FIT > 2048 / NT ? 2048 / NT : FIT);
 };
 
-// A pass over the region e: rows [LO, LO + RH), cut into NRP blocks of B
-// consecutive rows (thread row phase rp takes rows LO + rp B ...), and the
-// pair columns [PLO, PHI), the region's columns rounded out to whole pairs.
+// A pass over the region e: rows [LO, LO + RH) cut into NRP blocks of Q or
+// Q + 1 consecutive rows (the first REM row phases take the longer blocks;
+// thread row phase rp starts at r0(rp)), and the pair columns [PLO, PHI),
+// the region's columns rounded out to whole pairs.  Each thread walks Q rows
+// unconditionally plus at most one more, so the unrolled row loops carry no
+// per-row exit tests.
 template <int TX, int TY, int E, int NRP, int e>
 struct PairRegion {
-    static constexpr int LO = E - e, RH = TY + 2 * e, B = (RH + NRP - 1) / NRP;
+    static constexpr int LO = E - e, RH = TY + 2 * e, Q = RH / NRP, REM = RH % NRP;
     static constexpr int PLO = (E - e) >> 1, PHI = (E + TX + e + 1) >> 1;
+    static_assert(Q >= 1, "fewer region rows than row blocks");
+    __device__ static __forceinline__ int r0(int rp) { return LO + rp * Q + min(rp, REM); }
 };
+
+// Walks this thread's rows of the region with the 5-point window of `src`
+// (north / centre / south pairs in registers, west and east scalars loaded),
+// calling f(j, lap(src), centre pair, 2 * centre) for rows r0 + j.
+template <typename T, class Rg, int P, class F>
+__device__ __forceinline__ void pair_rows(const T* __restrict__ src, int rp, typename PairOf<T>::V i2x,
+                                          typename PairOf<T>::V i2y, F&& f) {
+    using V = typename PairOf<T>::V;
+    V n = p_ld(src - P), c = p_ld(src);
+    auto row = [&](int j) {
+        const V s = p_ld(src + (j + 1) * P);
+        const T w = src[j * P - 1], ee = src[j * P + 2];
+        V v2;
+        const V lap = p_lap(c, n, s, V{w, c.x}, V{c.y, ee}, i2x, i2y, &v2);
+        f(j, lap, c, v2);
+        n = c;
+        c = s;
+    };
+#pragma unroll
+    for (int j = 0; j < Rg::Q; ++j) row(j);
+    if (Rg::REM && rp < Rg::REM) row(Rg::Q);
+}
 
 // One mu pass: M = mu(Y) on the region e (rounded to pairs).
 template <typename T, int TX, int TY, int NRP, int e>
@@ -96,30 +128,17 @@ __device__ __forceinline__ void pair_mu_pass(const StageArgs<T>& S, const T* __r
     using V = typename PairOf<T>::V;
     constexpr int P = G::P;
     if (pc < Rg::PLO || pc >= Rg::PHI) return;
-    const int r0 = Rg::LO + rp * Rg::B;
-    const int nrows = min(Rg::B, Rg::LO + Rg::RH - r0);
-    if (nrows <= 0) return;
-    const T* y = Y + r0 * P + 2 * pc;
-    T* m = M + r0 * P + 2 * pc;
-    const V i2x = p_splat(S.i2[0]), i2y = p_splat(S.i2[1]);
+    const int off0 = Rg::r0(rp) * P + 2 * pc;
+    T* m = M + off0;
     const V two_rho = p_splat(S.p[2]), ca = p_splat(S.p[3]), cb = p_splat(S.p[4]);
     const V mk = p_splat(S.p[1]), one = p_splat((T)1), zero = p_splat((T)0);
-    V n = p_ld(y - P), c = p_ld(y);
-#pragma unroll
-    for (int j = 0; j < Rg::B; ++j) {
-        if (j >= nrows) break;
-        const V s = p_ld(y + (j + 1) * P);
-        const T w = y[j * P - 1], ee = y[j * P + 2];
-        V v2;
-        const V lap = p_lap(c, n, s, V{w, c.x}, V{c.y, ee}, i2x, i2y, &v2);
+    pair_rows<T, Rg, P>(Y + off0, rp, p_splat(S.i2[0]), p_splat(S.i2[1]), [&](int j, V lap, V c, V v2) {
         // f'(c) = (two_rho (c - ca)) (c - cb) ((2c - ca) - cb)   (f_dw)
         const V fa = p_mul(p_mul(two_rho, p_sub(c, ca)), p_sub(c, cb));
         const V fd = p_mul(fa, p_sub(p_sub(v2, ca), cb));
         // mu = (-kappa) lap + (1 f' + 0)   (PolCH::mu)
         p_st(m + j * P, p_fma(mk, lap, p_fma(one, fd, zero)));
-        n = c;
-        c = s;
-    }
+    });
 }
 
 // One k pass (stages 1-3): k = M lap(mu) + 0 on the region e; Y = u + a k
@@ -132,32 +151,21 @@ __device__ __forceinline__ void pair_k_pass(const StageArgs<T>& S, const T* __re
     using V = typename PairOf<T>::V;
     constexpr int P = G::P, E = G::E;
     if (pc < Rg::PLO || pc >= Rg::PHI) return;
-    const int r0 = Rg::LO + rp * Rg::B;
-    const int nrows = min(Rg::B, Rg::LO + Rg::RH - r0);
-    if (nrows <= 0) return;
+    const int r0 = Rg::r0(rp);
     const int off0 = r0 * P + 2 * pc;
-    const T* m = M + off0;
-    const V i2x = p_splat(S.i2[0]), i2y = p_splat(S.i2[1]);
     const V mob = p_splat(S.p[0]), zero = p_splat((T)0), av = p_splat(a), two = p_splat((T)2);
     const bool col_in = 2 * pc >= E && 2 * pc < E + TX;
-    V n = p_ld(m - P), c = p_ld(m);
-#pragma unroll
-    for (int j = 0; j < Rg::B; ++j) {
-        if (j >= nrows) break;
-        const V s = p_ld(m + (j + 1) * P);
-        const T w = m[j * P - 1], ee = m[j * P + 2];
-        V v2;
-        const V k = p_fma(mob, p_lap(c, n, s, V{w, c.x}, V{c.y, ee}, i2x, i2y, &v2), zero);
+    T* acc0 = ACC + (r0 - E) * TX + 2 * pc - E;  // dereferenced on tile rows only
+    pair_rows<T, Rg, P>(M + off0, rp, p_splat(S.i2[0]), p_splat(S.i2[1]), [&](int j, V lap, V, V) {
+        const V k = p_fma(mob, lap, zero);
         const int off = off0 + j * P;
         p_st(Y + off, p_fma(av, k, p_ld(U + off)));
         const int row = r0 + j;
         if (col_in && row >= E && row < E + TY) {
-            T* acc = ACC + (row - E) * TX + 2 * pc - E;
+            T* acc = acc0 + j * TX;
             p_st(acc, STAGE == 1 ? k : p_add(p_ld(acc), p_mul(two, k)));
         }
-        n = c;
-        c = s;
-    }
+    });
 }
 
 template <typename T, int TX, int TY, int NRP>
@@ -204,6 +212,26 @@ __device__ __forceinline__ void step_pair_tile(const StepArgs<T>& A, T* __restri
             if (ly < R) p_st(U + ly * P + 2 * pc, v[i]);
         }
     }
+    // the low parts of this thread's cells of the final update, fetched now
+    // so that their latency hides behind the four stages
+    using R0 = PairRegion<TX, TY, E, NRP, 0>;
+    const int fr0 = R0::r0(rp);
+    const int gx = x0 + 2 * pc - E;  // x of the pair's first cell in the final pass
+    const bool fcol = pc >= R0::PLO && pc < R0::PHI, x1 = gx + 1 < n0;
+    constexpr bool LO_STATE = sizeof(T) == 4;  // compensated state: FP32 steppers only
+    V lo_pf[LO_STATE ? R0::Q + 1 : 1];
+    if constexpr (LO_STATE) {
+#pragma unroll
+        for (int j = 0; j <= R0::Q; ++j) {
+            lo_pf[j] = p_splat((T)0);
+            const int py = y0 + fr0 + j - E;
+            if (S.ulo[0] && fcol && (j < R0::Q || rp < R0::REM) && py < n1 && gx < n0) {
+                const T* g = S.ulo[0] + L.origin + gx + L.s[1] * py;
+                lo_pf[j].x = __ldg(g);
+                if (x1) lo_pf[j].y = __ldg(g + 1);
+            }
+        }
+    }
     __syncthreads();
 
     // stage 1: y1 = u
@@ -226,57 +254,42 @@ __device__ __forceinline__ void step_pair_tile(const StepArgs<T>& A, T* __restri
     __syncthreads();
 
     // k4 on the tile, then u' = u + dt/6 (((k1 + 2 k2) + 2 k3) + k4)
-    {
-        using Rg = PairRegion<TX, TY, E, NRP, 0>;
-        const int r0 = Rg::LO + rp * Rg::B;
-        const int nrows = min(Rg::B, Rg::LO + Rg::RH - r0);
-        if (pc >= Rg::PLO && pc < Rg::PHI && nrows > 0) {
-            const int off0 = r0 * P + 2 * pc;
-            const T* m = M + off0;
-            const V i2x = p_splat(S.i2[0]), i2y = p_splat(S.i2[1]);
-            const V mob = p_splat(S.p[0]), zero = p_splat((T)0), dtf = p_splat(S.dtf);
-            const int gx = x0 + 2 * pc - E;  // x of the pair's first cell
-            const bool x1 = gx + 1 < n0;
-            V n = p_ld(m - P), c = p_ld(m);
-#pragma unroll
-            for (int j = 0; j < Rg::B; ++j) {
-                if (j >= nrows) break;
-                const V s = p_ld(m + (j + 1) * P);
-                const T w = m[j * P - 1], ee = m[j * P + 2];
-                V v2;
-                const V k = p_fma(mob, p_lap(c, n, s, V{w, c.x}, V{c.y, ee}, i2x, i2y, &v2), zero);
-                n = c;
-                c = s;
-                const int row = r0 + j, py = y0 + row - E;
-                if (py >= n1 || gx >= n0) break;  // past the grid (partial tiles)
-                const V sum = p_add(p_ld(ACC + (row - E) * TX + 2 * pc - E), k);
+    if (fcol) {
+        const V mob = p_splat(S.p[0]), zero = p_splat((T)0), dtf = p_splat(S.dtf);
+        const int off0 = fr0 * P + 2 * pc;
+        pair_rows<T, R0, P>(M + off0, rp, p_splat(S.i2[0]), p_splat(S.i2[1]), [&](int j, V lap, V, V) {
+            const V k = p_fma(mob, lap, zero);
+            const int py = y0 + fr0 + j - E;
+            if (py < n1 && gx < n0) {  // inside the grid (partial tiles)
+                const V sum = p_add(p_ld(ACC + (fr0 + j - E) * TX + 2 * pc - E), k);
                 const V u = p_ld(U + off0 + j * P);
-                const V d = p_mul(dtf, sum);
                 const int idx = L.origin + gx + L.s[1] * py;
-                if (S.ulo[0]) {
-                    twosum_update(u.x, __ldg(S.ulo[0] + idx), d.x, &S.out[0][idx], &S.outlo[0][idx]);
-                    if (x1) twosum_update(u.y, __ldg(S.ulo[0] + idx + 1), d.y, &S.out[0][idx + 1],
-                                          &S.outlo[0][idx + 1]);
+                if (LO_STATE && S.ulo[0]) {
+                    const V d = p_mul(dtf, sum);
+                    const V l = lo_pf[LO_STATE ? j : 0];
+                    twosum_update(u.x, l.x, d.x, &S.out[0][idx], &S.outlo[0][idx]);
+                    if (x1) twosum_update(u.y, l.y, d.y, &S.out[0][idx + 1], &S.outlo[0][idx + 1]);
                 } else {
                     const V o = p_fma(dtf, sum, u);
                     S.out[0][idx] = o.x;
                     if (x1) S.out[0][idx + 1] = o.y;
                 }
             }
-        }
+        });
     }
     if (!inside) box_ghosts<T, 2, 1, TX, TY, G::NT>(S, x0, y0);
 }
 
 template <typename T, int TX, int TY, int NRP>
-__global__ void __launch_bounds__(StepPair<T, TX, TY, NRP>::NT) step_pair(const StepArgs<T> A) {
+__global__ void __launch_bounds__(StepPair<T, TX, TY, NRP>::NT, StepPair<T, TX, TY, NRP>::MINB)
+    step_pair(const StepArgs<T> A) {
     extern __shared__ __align__(16) unsigned char step_smem[];
     step_pair_tile<T, TX, TY, NRP>(A, reinterpret_cast<T*>(step_smem), blockIdx.x * TX, blockIdx.y * TY);
 }
 
 // Many fields in one launch: one CTA per entry of the tile list.
 template <typename T, int TX, int TY, int NRP>
-__global__ void __launch_bounds__(StepPair<T, TX, TY, NRP>::NT)
+__global__ void __launch_bounds__(StepPair<T, TX, TY, NRP>::NT, StepPair<T, TX, TY, NRP>::MINB)
     step_pair_batched(const StepArgs<T>* __restrict__ args, const BatchTile* __restrict__ tiles) {
     extern __shared__ __align__(16) unsigned char step_smem[];
     const BatchTile bt = tiles[blockIdx.x];
