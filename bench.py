@@ -135,9 +135,23 @@ WORKLOADS = {
 # captures summarised under profiles/ (cold L2, so an upper bound for the
 # graph-replayed launches); keyed by (workload, dtype, launches per time step).
 TRAFFIC = {
-    ("ch2d", "f64", 4): 12.63e6,  # profiles/stage_box_ch1024_f64.md: mean of stage 1 and 2 launches
-    ("ch2d", "f32", 1): 8.47e6,   # profiles/step_box_ch1024_f32.md
+    ("ch2d", "f64", "step_pair"): 8.46e6,   # profiles/step_pair_ch1024_f64.md
+    ("ch2d", "f32", "step_pair"): 8.46e6,   # profiles/step_pair_ch1024_f32.md
+    ("ch2d", "f64", "stage_box"): 12.63e6,  # profiles/stage_box_ch1024_f64.md: mean of stage 1 and 2 launches
+    ("ch2d", "f32", "step_box"): 8.47e6,    # profiles/step_box_ch1024_f32.md
+    ("batch", "f32", "step_pair_batched"): 358.3e6,  # profiles/step_pair_batched_batch64_f32.md
 }
+
+# step tiles 6 and up are the pair kernels (include/phix_b200.h, phix_stepper_set_tiles)
+FIRST_PAIR_TILE = 6
+
+
+def dominant_kernel(px, g, phys, scheme, lps, fused, tile):
+    """Name of the kernel that takes the time step (the key of TRAFFIC)."""
+    periodic_ch = phys == px.PHYS_CH and g.dim == 2 and all(g.bc_type[i] == px.BC_PERIODIC for i in range(4))
+    if lps == 1 and scheme == px.RK4 and fused:
+        return "step_pair" if (tile >= FIRST_PAIR_TILE or (tile == -1 and periodic_ch)) else "step_box"
+    return "stage_box" if tile == -1 else "stage_col"
 
 
 class StepperRun:
@@ -172,6 +186,7 @@ class StepperRun:
         fused, tile = self.st.tiles()
         self.launch = {"one_launch_per_time_step": fused, "tile_cfg": tile}
         self.lps = self.st.launches_per_step
+        self.kernel = dominant_kernel(px, g, phys, scheme, self.lps, fused, tile)
         self.st.set_graph(self.K)
         self.h_in = [torch.from_numpy(f).pin_memory() for f in fields]
         self.h_out = [torch.empty_like(h).pin_memory() for h in self.h_in]
@@ -221,6 +236,9 @@ class BatchRun:
             if args.launch == "stage":
                 self.b.set_fusion(False)
         self.lps = self.b.launches_per_step
+        periodic = all(g.bc_type[i] == px.BC_PERIODIC for g in grids for i in range(4))
+        self.kernel = ("step_pair_batched" if periodic and phys == px.PHYS_CH else "step_box_batched") \
+            if self.lps == 1 else "stage_box_batched"
         self.b.set_graph(self.K)
         self.h_in = [torch.from_numpy(f).pin_memory() for f in fields]
         self.h_out = [torch.empty_like(h).pin_memory() for h in self.h_in]
@@ -399,7 +417,8 @@ def bench_ours(args):
                        "parallelism": (f"instances bin-packed over {world} ranks" if args.workload == "batch"
                                        else f"replicas x{world}")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": TRAFFIC.get((args.workload, args.dtype, run.lps)),
+                         "frac": achieved / peak, "traffic": TRAFFIC.get((args.workload, args.dtype, run.kernel)),
+                         "kernel": run.kernel,
                          "note": f"algorithmic {per_cell} B per field-cell update over the CUDA-event time of "
                                  f"one time step ({run.lps} launch{'es' if run.lps > 1 else ''} per time step); "
                                  f"peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs); traffic = ncu DRAM bytes per "

@@ -309,11 +309,12 @@ int prepare_stage(int phys, int dim, int prec) {
 
 // Pair tile for a grid: among the shapes with at least two resident CTAs
 // and 1024 (FP32) or 512 (FP64) resident threads per SM (fewer leave too few
-// warps to hide the barriers' latency), the least (waves x CTAs per SM x
-// work per tile), work per tile being the cells of the eight passes'
-// regions; ties go to the earlier shape.  On B200 this picks 128x28 (FP32)
-// and 64x28 (FP64) at 1024^2 and 128x32 for FP32 at 4096^2, the fastest
-// measured there.
+// warps to hide the barriers' latency), the least (tiles per SM, rounded up)
+// x (work per tile), work per tile being the cells of the eight passes'
+// regions; ties go to the earlier shape.  Grids that do not fill the SMs
+// get smaller tiles spread over more of them.  On B200 this picks 128x28
+// (FP32) and 64x28 (FP64) at 1024^2 and 128x32 for FP32 at 4096^2, the
+// fastest measured there.
 template <typename T>
 int pick_pair_cfg(const Layout& L, int nsm) {
     int best = 1;
@@ -324,10 +325,9 @@ int pick_pair_cfg(const Layout& L, int nsm) {
         const int tx = kPairCfgs[i][0], ty = kPairCfgs[i][1];
         if (occ * (tx / 2 + 8) * kPairCfgs[i][2] < (sizeof(T) == 4 ? 1024 : 512)) continue;
         const double tiles = (double)((L.n[0] + tx - 1) / tx) * ((L.n[1] + ty - 1) / ty);
-        const double waves = std::ceil(tiles / ((double)nsm * occ));
         double work = 0.0;
         for (int e = 0; e <= 7; ++e) work += (double)(tx + 2 * e + (e & 1)) * (ty + 2 * e);
-        const double cost = waves * occ * work;
+        const double cost = std::ceil(tiles / nsm) * work;
         if (cost < best_cost) { best_cost = cost; best = i; }
     }
     return best;
