@@ -468,6 +468,7 @@ def bench_surrogate(args):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     launches0 = px.launch_count()
     with ClockSampler(dev.index) as clk:
+        torch.cuda.nvtx.range_push("timed")  # profilers select the timed launches by this range
         for i in range(args.steps):
             ev[i][0].record(stream)
             for _ in range(SUR_K):
@@ -475,6 +476,7 @@ def bench_surrogate(args):
                 a, b = b, a
             ev[i][1].record(stream)
             flush_l2(flush)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize(dev)
     launches = px.launch_count() - launches0
     total_ms = sum(s_.elapsed_time(e_) for s_, e_ in ev)

@@ -251,7 +251,8 @@ int phix_batch_mass(phix_batch_t* b, double* masses);
  * predicts c(t + 50 dt) - c(t) from c(t), followed by an exact FP64
  * mean-mass projection.  The 32 -> 32 layers (forward, data gradient and
  * weight gradient) run as BF16 implicit GEMMs on the tcgen05 tensor cores
- * with FP32 accumulation in TMEM.  States are compact [B][H][W] FP64 device
+ * with FP32 accumulation in TMEM; the fused inference step runs the 1 -> 32
+ * and 32 -> 1 layers as UMMAs as well.  States are compact [B][H][W] FP64 device
  * arrays; W must be a multiple of 128.  No reference counterpart: the
  * reference only has the FD solver (Solver.cu). */
 typedef struct phix_surrogate phix_surrogate_t;
@@ -263,8 +264,15 @@ int phix_surrogate_destroy(phix_surrogate_t* s);
 int phix_surrogate_nparams(void);
 int phix_surrogate_set_params(phix_surrogate_t* s, const float* host_params);
 int phix_surrogate_get_params(phix_surrogate_t* s, float* host_params, float* host_grads);
-/* c_out = c + out_scale * net(c), then c_out += mean(c) - mean(c_out). */
+/* c_out = c + out_scale * net(c), then c_out += mean(c) - mean(c_out).  By
+ * default one fused kernel (all four layers on the tensor cores, layers 1
+ * and 4 as UMMAs too, activations never leaving shared memory) plus the
+ * projection; c and c_out must not overlap. */
 int phix_surrogate_step(phix_surrogate_t* s, const double* c, double* c_out, int B, void* stream);
+/* 1 (default): phix_surrogate_step runs the fused kernel; 0: the per-layer
+ * kernels of phix_surrogate_forward (layers 1 and 4 on CUDA cores).  The two
+ * agree to FP32 rounding of the thin layers' sums.  No reference counterpart. */
+int phix_surrogate_set_fused(phix_surrogate_t* s, int on);
 /* Raw network output o = net(c) as FP32 [B][H][W]. */
 int phix_surrogate_forward(phix_surrogate_t* s, const double* c, float* o, int B, void* stream);
 /* Gradient of mean((o - (c_next - c)/out_scale)^2) into the internal

@@ -133,6 +133,7 @@ def lib() -> C.CDLL:
         "phix_surrogate_set_params": ([vp, vp], C.c_int),
         "phix_surrogate_get_params": ([vp, vp, vp], C.c_int),
         "phix_surrogate_step": ([vp, vp, vp, C.c_int, vp], C.c_int),
+        "phix_surrogate_set_fused": ([vp, C.c_int], C.c_int),
         "phix_surrogate_forward": ([vp, vp, vp, C.c_int, vp], C.c_int),
         "phix_surrogate_grad": ([vp, vp, vp, C.c_int, P, vp], C.c_int),
         "phix_surrogate_adam": ([vp, vp, C.c_float, vp], C.c_int),
@@ -444,6 +445,10 @@ class Surrogate:
         g = np.empty(self.nparams, np.float32)
         check(lib().phix_surrogate_get_params(self.h, C.c_void_p(p.ctypes.data), C.c_void_p(g.ctypes.data)))
         return p, g
+
+    def set_fused(self, on: bool):
+        """step(): one fused kernel (True, default) or the per-layer kernels."""
+        check(lib().phix_surrogate_set_fused(self.h, 1 if on else 0))
 
     def step(self, c, c_out, stream=None):
         check(lib().phix_surrogate_step(self.h, C.c_void_p(c.data_ptr()), C.c_void_p(c_out.data_ptr()),

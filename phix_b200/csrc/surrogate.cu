@@ -643,6 +643,308 @@ __global__ void __launch_bounds__(256) apply_correction(double* __restrict__ c_o
         c_out[img * npix + p] += cr;
 }
 
+// ---------------------------------------------------------------------------
+// One surrogate step in one kernel (inference)
+// ---------------------------------------------------------------------------
+// Each CTA takes a window of FW output pixels of one image and a strip of
+// output rows, and streams the strip's rows through the four layers, all on
+// the tensor cores: layer 1 as one UMMA (M128 N32 K16) over a 9-tap im2col
+// tile, layers 2 and 3 as 18 UMMAs (M128 N32 K16), layer 4 as 18 UMMAs
+// (M128 N16 K16, output channel 0 of 16; the other 15 weight rows are zero).
+// The CUDA cores build the im2col tiles and run the epilogues.
+//
+// Ticks.  At tick t one thread issues this tick's UMMAs into TMEM
+// accumulator set t & 1 while all threads run the epilogues of tick t - 1's
+// UMMAs (set (t - 1) & 1), so the tensor cores and the epilogues overlap:
+//   tick t UMMAs:      layer 1 -> row Y-4+t, layer 2 -> Y-7+t,
+//                      layer 3 -> Y-10+t, layer 4 -> Y-13+t;
+//   tick t epilogues:  the rows of tick t - 1;  im2col of row Y-3+t.
+// A layer reads rows whose epilogues ran by the previous tick, so a strip of
+// R output rows takes R + 14 ticks.  Activations live in rings of 5 staged
+// rows ([8-channel chunk][130 px][8], as conv32_rows_tc's input rows): a row
+// is read by the UMMAs of the three ticks after its epilogue, and the last of
+// those completes before the epilogue that reuses its slot.
+//
+// Window pixels: a window with first output pixel X computes layer 1 on
+// x = X-3 .. X+124, layer 2 on X-2 .., layer 3 on X-1 .., and keeps layer 4
+// on X .. X+FW-1 (each 128-wide UMMA row loses one valid pixel at each side
+// per layer).  c_out = c + out_scale * o is written without the mass
+// projection; each CTA's FP64 sums of c and c_out go to part[job] and
+// finish_projection applies the correction.
+constexpr int FW = 122;                      // output pixels per window
+constexpr int F_EW = 16;                     // epilogue warps: TMEM lane quadrant (w % 4), 8-channel chunk (w / 4)
+constexpr int F_NT = 32 * (F_EW + 1);        // + one warp that issues the UMMAs
+constexpr int IM_B = 2 * TILE * 16;          // 4096: im2col tile [k chunk][128 px][8] bf16 (taps 0-7 | 8, 0..)
+constexpr int W1PK_B = 2 * 32 * 16;          // 1024: layer-1 weights [k chunk][32 n][8]
+constexpr int W4PK_B = 9 * 2 * 2 * 16 * 16;  // 9216: layer-4 weights [tap][k16][chunk][16 n][8]
+constexpr int F_RING = 5, F_IMS = 3;
+constexpr int F_H1 = 0, F_H2 = F_H1 + F_RING * ROW_B, F_H3 = F_H2 + F_RING * ROW_B, F_IM = F_H3 + F_RING * ROW_B,
+              F_W2 = F_IM + F_IMS * IM_B, F_W3 = F_W2 + WPK_B, F_W1 = F_W3 + WPK_B, F_W4 = F_W1 + W1PK_B,
+              F_BAR = F_W4 + W4PK_B, F_SMEM = F_BAR + 128;
+static_assert(F_SMEM <= 227 * 1024, "fused step exceeds shared memory");
+
+// GELU (tanh form) of two values on the packed f32x2 instructions:
+// 0.5 x (1 + tanh(k (x + c x^3))), with h = 0.5 x and y = fma(h, t, h).
+__device__ __forceinline__ float2 gelu2(float2 x) {
+    const float2 x2 = __fmul2_rn(x, x);
+    const float2 in = __ffma2_rn(__fmul2_rn(make_float2(0.044715f, 0.044715f), x2), x, x);
+    const float2 u = __fmul2_rn(make_float2(0.7978845608028654f, 0.7978845608028654f), in);
+    const float2 t = make_float2(tanh_hw(u.x), tanh_hw(u.y));
+    const float2 h = __fmul2_rn(make_float2(0.5f, 0.5f), x);
+    return __ffma2_rn(h, t, h);
+}
+
+struct FusedArgs {
+    const double* c;
+    double* c_out;
+    const __nv_bfloat16* wpk;   // layer-2 forward pack, then layer 3's (9216 elements each)
+    const __nv_bfloat16* thin;  // layer-1 pack (512 elements), then layer 4's (4608)
+    const float *b1, *b2, *b3, *b4;
+    double* part;               // [job][2]: sums of c and c_out over the job's output pixels
+    int* err;
+    int H, W, nwin, nstrip, rows;
+    NetParams P;
+};
+
+__device__ __forceinline__ int fring(int q) { return (q % F_RING + F_RING) % F_RING; }
+
+__global__ void __launch_bounds__(F_NT, 1) step_fused_tc(const FusedArgs a) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + F_BAR);  // [layer][set]
+    uint32_t* slot_t = reinterpret_cast<uint32_t*>(sm + F_BAR + 64);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int job = blockIdx.x;
+    const int b = job / (a.nwin * a.nstrip), rem = job - b * a.nwin * a.nstrip;
+    const int win = rem / a.nstrip, strip = rem - win * a.nstrip;
+    const int X = win * FW, Y = strip * a.rows, R = min(a.rows, a.H - Y);
+
+    // weights in, rings and im2col tiles zeroed (the two pixels past each
+    // 128-pixel row are read by the UMMAs but never written)
+    {
+        const uint4* w = reinterpret_cast<const uint4*>(a.wpk);
+        uint4* d = reinterpret_cast<uint4*>(sm + F_W2);
+        for (int u = threadIdx.x; u < 2 * WPK_B / 16; u += F_NT) d[u] = __ldg(w + u);
+        const uint4* th = reinterpret_cast<const uint4*>(a.thin);
+        uint4* dt = reinterpret_cast<uint4*>(sm + F_W1);
+        for (int u = threadIdx.x; u < (W1PK_B + W4PK_B) / 16; u += F_NT) dt[u] = __ldg(th + u);
+        uint4* z = reinterpret_cast<uint4*>(sm);
+        for (int u = threadIdx.x; u < F_W2 / 16; u += F_NT) z[u] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(slot_t, 256);
+        tc::tmem_relinquish();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 8; ++k) tc::mbar_init(bar + k, 1);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot_t;
+    const uint32_t id32 = tc::idesc_bf16_f32(128, 32, 0, 0), id16 = tc::idesc_bf16_f32(128, 16, 0, 0);
+    const uint32_t sa = tc::smem_u32(sm);
+    const uint64_t w1d = tc::sdesc(sa + F_W1, 512, 128), w2d = tc::sdesc(sa + F_W2, 512, 128),
+                   w3d = tc::sdesc(sa + F_W3, 512, 128), w4d = tc::sdesc(sa + F_W4, 256, 128);
+    const int quad = warp & 3, chunk = warp >> 2;
+    const bool ew = warp < F_EW;  // an epilogue warp
+    float2 bias1[4], bias2[4], bias3[4];
+    const int bc = ew ? 8 * chunk : 0;  // the issue warp loads (and never uses) chunk 0's
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        bias1[n] = make_float2(__ldg(a.b1 + bc + 2 * n), __ldg(a.b1 + bc + 2 * n + 1));
+        bias2[n] = make_float2(__ldg(a.b2 + bc + 2 * n), __ldg(a.b2 + bc + 2 * n + 1));
+        bias3[n] = make_float2(__ldg(a.b3 + bc + 2 * n), __ldg(a.b3 + bc + 2 * n + 1));
+    }
+    const float b4 = __ldg(a.b4);
+    uint32_t phase[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+    uint32_t pending = 0u;  // barriers with a commit not yet waited for (thread 0's copy, which waits on all, is used)
+    bool failed = false;
+    double sc = 0.0, so = 0.0;
+
+    // rows of tick t: layer 1, 2, 3, 4 and whether each is in its range
+    auto row_of = [&](int k, int t) { return Y - (k == 0 ? 4 : k == 1 ? 7 : k == 2 ? 10 : 13) + t; };
+    auto live = [&](int k, int t) {
+        return k == 0 ? (t >= 1 && t < R + 7) : k == 1 ? (t >= 5 && t < R + 9) : k == 2 ? (t >= 9 && t < R + 11)
+                                                                                      : (t >= 13 && t < R + 13);
+    };
+    // GELU epilogue of a 32-channel accumulator (TMEM column col) into the
+    // staged row of ring `off` for row r: pixel quad*32 + lane, channels
+    // 8*chunk .. 8*chunk + 7
+    auto act_row = [&](uint32_t col, const float2* bias, int off, int r) {
+        float v[8];
+        tc::tmem_ld8(tmem + ((uint32_t)(quad * 32) << 16) + col + (uint32_t)(8 * chunk), v);
+        uint32_t pk[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const float2 g = gelu2(__fadd2_rn(make_float2(v[2 * n], v[2 * n + 1]), bias[n]));
+            pk[n] = pack2(g.x, g.y);
+        }
+        *reinterpret_cast<uint4*>(sm + off + fring(r) * ROW_B + chunk * CHUNK_B + (quad * 32 + lane) * 16) =
+            make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    };
+    // warp-uniform, so that a warp either runs its tcgen05.ld whole or not at all
+    auto wait = [&](int k) {
+        const bool ok = __all_sync(0xffffffffu, tc::mbar_wait_bounded(bar + k, phase[k], WAIT_NS));
+        if (!ok) {
+            failed = true;
+            return false;
+        }
+        phase[k] ^= 1u;
+        pending &= ~(1u << k);
+        tc::fence_after_sync();
+        return true;
+    };
+
+    const int nticks = R + 14;
+    for (int t = 0; t < nticks; ++t) {
+        const int set = t & 1;
+        const uint32_t tset = tmem + (uint32_t)(128 * set);
+        if (warp == F_EW && lane == 0) {
+            // Shared-memory descriptors are linear in the address (bits 0-13 =
+            // address / 16, no carry below 256 KB), so each UMMA's descriptors
+            // are a per-row base plus a compile-time offset.
+            if (live(0, t)) {
+                const uint64_t ad = tc::sdesc(sa + F_IM + ((t - 1) % F_IMS) * IM_B, TILE * 16, 128);
+                tc::umma_bf16(tset, ad, w1d, id32, 0);
+                tc::umma_commit(bar + 0 * 2 + set);
+            }
+            auto conv = [&](int in_off, uint64_t wd, int r, uint32_t col, uint32_t id, int wblk) {
+                uint64_t rd[3];
+#pragma unroll
+                for (int ky = 0; ky < 3; ++ky) rd[ky] = tc::sdesc(sa + in_off + fring(r - 1 + ky) * ROW_B, CHUNK_B, 128);
+#pragma unroll
+                for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk) {
+                        const int ky = tap / 3, kx = tap % 3;
+                        const uint64_t ad = rd[ky] + (uint64_t)((2 * kk * CHUNK_B + kx * 16) >> 4);
+                        const uint64_t bd = wd + (uint64_t)(((tap * 2 + kk) * wblk) >> 4);
+                        tc::umma_bf16(tset + col, ad, bd, id, (tap | kk) != 0);
+                    }
+            };
+            if (live(1, t)) { conv(F_H1, w2d, row_of(1, t), 32, id32, 1024); tc::umma_commit(bar + 1 * 2 + set); }
+            if (live(2, t)) { conv(F_H2, w3d, row_of(2, t), 64, id32, 1024); tc::umma_commit(bar + 2 * 2 + set); }
+            if (live(3, t)) { conv(F_H3, w4d, row_of(3, t), 96, id16, 512); tc::umma_commit(bar + 3 * 2 + set); }
+        }
+        for (int k = 0; k < 4; ++k)
+            if (live(k, t)) pending |= 1u << (2 * k + set);
+        // im2col of layer-1 row Y-3+t for the next tick (pixel m <-> x = X-3+m):
+        // the c values are loaded now and stored after the epilogues
+        const bool im = ew && t < R + 6 && threadIdx.x < TILE;
+        double cv9[9];
+        if (im) {
+            const int m = threadIdx.x, ry = Y - 3 + t, x = X - 3 + m;
+#pragma unroll
+            for (int k = 0; k < 9; ++k)
+                cv9[k] = __ldg(a.c + ((size_t)b * a.H + wrap(ry - 1 + k / 3, a.H)) * a.W + wrap(x - 1 + k % 3, a.W));
+        }
+        // epilogues of the previous tick's UMMAs
+        const int e = t - 1, es = e & 1;
+        const uint32_t eset = (uint32_t)(128 * es);
+        if (ew && e >= 0) {
+            if (live(0, e) && !failed && wait(0 * 2 + es)) act_row(eset + 0, bias1, F_H1, row_of(0, e));
+            if (live(1, e) && !failed && wait(1 * 2 + es)) act_row(eset + 32, bias2, F_H2, row_of(1, e));
+            if (live(2, e) && !failed && wait(2 * 2 + es)) act_row(eset + 64, bias3, F_H3, row_of(2, e));
+            if (live(3, e) && !failed && wait(3 * 2 + es) && chunk == 0) {
+                float v[8];
+                tc::tmem_ld8(tmem + ((uint32_t)(quad * 32) << 16) + eset + 96u, v);
+                const int m = quad * 32 + lane, x = X + m;
+                if (m < FW && x < a.W) {
+                    const size_t p = ((size_t)b * a.H + row_of(3, e)) * a.W + x;
+                    const float o = v[0] + b4;
+                    const double cv = __ldg(a.c + p), co = cv + a.P.out_scale * (double)o;
+                    a.c_out[p] = co;
+                    sc += cv;
+                    so += co;
+                }
+            }
+        }
+        if (im) {  // x0 = bf16((c - in_shift) * in_scale), as layer1_fwd's x0_at
+            float v[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k)
+                v[k] = __bfloat162float(__float2bfloat16_rn((float)((cv9[k] - a.P.in_shift) * a.P.in_scale)));
+            uint8_t* dst = sm + F_IM + (t % F_IMS) * IM_B + threadIdx.x * 16;
+            *reinterpret_cast<uint4*>(dst) =
+                make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+            *reinterpret_cast<uint4*>(dst + TILE * 16) = make_uint4(pack2(v[8], 0.f), 0u, 0u, 0u);
+        }
+        // generic-proxy ring writes -> the next tick's UMMAs
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        if (__syncthreads_or(failed)) {
+            failed = true;
+            break;
+        }
+        tc::fence_after_sync();
+    }
+    // a failed CTA may leave UMMAs in flight: wait (bounded) for the last
+    // commit of each barrier before the TMEM is released
+    if (failed && threadIdx.x == 0)
+        for (int k = 0; k < 8; ++k)
+            if (pending & (1u << k)) tc::mbar_wait_bounded(bar + k, phase[k], WAIT_NS);
+
+    __shared__ double red[2][F_NT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sc += __shfl_xor_sync(0xffffffffu, sc, o);
+        so += __shfl_xor_sync(0xffffffffu, so, o);
+    }
+    if (lane == 0) { red[0][warp] = sc; red[1][warp] = so; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int w = 0; w < F_NT / 32; ++w) { s0 += red[0][w]; s1 += red[1][w]; }
+        a.part[2 * job] = s0;
+        a.part[2 * job + 1] = s1;
+        if (failed) atomicExch(a.err, 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 256);
+}
+
+// The mean-mass projection after step_fused_tc: every block sums its image's
+// job partials in the same fixed order, then adds the correction to its
+// share of the image's pixels.
+__global__ void __launch_bounds__(256) finish_projection(double* __restrict__ c_out, const double* __restrict__ part,
+                                                         int jobs_per_img, size_t npix) {
+    const int img = blockIdx.y;
+    __shared__ double corr_s;
+    if (threadIdx.x < 32) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int j = threadIdx.x; j < jobs_per_img; j += 32) {
+            s0 += part[2 * ((size_t)img * jobs_per_img + j)];
+            s1 += part[2 * ((size_t)img * jobs_per_img + j) + 1];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        }
+        if (threadIdx.x == 0) corr_s = (s0 - s1) / (double)npix;
+    }
+    __syncthreads();
+    const double cr = corr_s;
+    for (size_t p = blockIdx.x * 256ull + threadIdx.x; p < npix; p += (size_t)gridDim.x * 256)
+        c_out[img * npix + p] += cr;
+}
+
+// Layer-1 and layer-4 operands of step_fused_tc (bf16):
+//   thin[0 .. 511]      [k chunk][32 n][8]              = W1[n][8 chunk + e] (taps 9..15: 0)
+//   thin[512 .. 5119]   [tap][k16][chunk][16 n][8]      = W4[tap][16 k16 + 8 chunk + e] for n = 0, else 0
+__global__ void pack_thin(const float* __restrict__ W1, const float* __restrict__ W4, __nv_bfloat16* __restrict__ thin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 512) {
+        const int e = i % 8, n = (i / 8) % 32, kc = i / 256, k = 8 * kc + e;
+        thin[i] = __float2bfloat16_rn(k < 9 ? W1[n * 9 + k] : 0.f);
+    } else if (i < 512 + 4608) {
+        const int r = i - 512;
+        const int e = r % 8, n = (r / 8) % 16, chunk = (r / 128) % 2, kk = (r / 256) % 2, tap = r / 512;
+        thin[i] = __float2bfloat16_rn(n == 0 ? W4[tap * 32 + 16 * kk + 8 * chunk + e] : 0.f);
+    }
+}
+
 // Per-image FP64 sums of a and b (grid-stride per image: one block row per image).
 __global__ void __launch_bounds__(256) image_sums(const double* __restrict__ a, const double* __restrict__ bb,
                                                   size_t npix, double* __restrict__ out) {
@@ -898,6 +1200,8 @@ struct phix_surrogate {
     double* lpart = nullptr;
     int* err = nullptr;
     bool packed = false;
+    __nv_bfloat16* thin = nullptr;  // layer-1 and layer-4 UMMA operands of the fused step
+    bool fused = true;              // phix_surrogate_step: one fused kernel (else the layer kernels)
 };
 
 namespace {
@@ -913,6 +1217,8 @@ int sg_pack(phix_surrogate* s, cudaStream_t st) {
     pack_weights<<<(total + 255) / 256, 256, 0, st>>>(s->params + OFF_W2, s->params + OFF_W3, s->params + OFF_W1,
                                                       s->params + OFF_W4, s->pk, s->w1r, s->w4r);
     PHIX_LAUNCH_CHECK("pack_weights");
+    pack_thin<<<(512 + 4608 + 255) / 256, 256, 0, st>>>(s->params + OFF_W1, s->params + OFF_W4, s->thin);
+    PHIX_LAUNCH_CHECK("pack_thin");
     s->packed = true;
     return PHIX_OK;
 }
@@ -932,10 +1238,36 @@ int sg_conv_rows(phix_surrogate* s, const ConvArgs& a, cudaStream_t st) {
     return PHIX_OK;
 }
 
+// One surrogate step as step_fused_tc + finish_projection: strips of
+// ceil(B * windows * H / SMs) rows, so the jobs fill one wave of one CTA per SM.
+int sg_step_fused(phix_surrogate* s, const double* c, int B, double* c_out, cudaStream_t st) {
+    FusedArgs a{};
+    a.c = c; a.c_out = c_out; a.wpk = s->pk; a.thin = s->thin;
+    a.b1 = s->params + OFF_B1; a.b2 = s->params + OFF_B2; a.b3 = s->params + OFF_B3; a.b4 = s->params + OFF_B4;
+    a.part = s->sums; a.err = s->err;
+    a.H = s->H; a.W = s->W; a.P = s->P;
+    a.nwin = (s->W + FW - 1) / FW;
+    const long long rows_total = (long long)B * a.nwin * s->H;
+    a.rows = (int)((rows_total + s->nsm - 1) / s->nsm);
+    if (a.rows < 1) a.rows = 1;
+    a.nstrip = (s->H + a.rows - 1) / a.rows;
+    const int jobs_per_img = a.nwin * a.nstrip, njobs = B * jobs_per_img;
+    step_fused_tc<<<njobs, F_NT, F_SMEM, st>>>(a);
+    PHIX_LAUNCH_CHECK("step_fused_tc");
+    const size_t npix = (size_t)s->H * s->W;
+    int pb = (int)((npix + 255) / 256);
+    const int pmax = (s->nsm * 4 + B - 1) / B;
+    pb = pb < pmax ? pb : pmax;
+    finish_projection<<<dim3(pb, B), 256, 0, st>>>(c_out, s->sums, jobs_per_img, npix);
+    PHIX_LAUNCH_CHECK("finish_projection");
+    return PHIX_OK;
+}
+
 int sg_forward(phix_surrogate* s, const double* c, int B, double* c_out, float* o_out, cudaStream_t st,
                bool keep_z = true) {
     int rc;
     if (!s->packed && (rc = sg_pack(s, st))) return rc;
+    if (s->fused && c_out && !o_out && !keep_z) return sg_step_fused(s, c, B, c_out, st);
     const size_t N = (size_t)B * s->H * s->W;
     const int eg = (int)((N + 255) / 256 < (size_t)s->nsm * 8 ? (N + 255) / 256 : (size_t)s->nsm * 8);
     layer1_fwd<<<eg, 256, 0, st>>>(c, s->w1r, s->params + OFF_B1, keep_z ? s->z1 : nullptr, s->h1, B, s->H, s->W,
@@ -986,6 +1318,8 @@ int phix_surrogate_create(phix_surrogate_t** out, int H, int W, int batch_max, d
         if (ea != cudaSuccess) { delete s; return cuda_status(ea, "cudaFuncSetAttribute(wgrad)"); }
         ea = cudaFuncSetAttribute(conv32_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROWS_SMEM);
         if (ea != cudaSuccess) { delete s; return cuda_status(ea, "cudaFuncSetAttribute(conv rows)"); }
+        ea = cudaFuncSetAttribute(step_fused_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, F_SMEM);
+        if (ea != cudaSuccess) { delete s; return cuda_status(ea, "cudaFuncSetAttribute(fused step)"); }
     }
     s->P.in_shift = in_shift; s->P.in_scale = in_scale; s->P.out_scale = out_scale;
     int dev = 0;
@@ -998,6 +1332,7 @@ int phix_surrogate_create(phix_surrogate_t** out, int H, int W, int batch_max, d
     A((void**)&s->params, NPARAM * 4); A((void**)&s->grads, NPARAM * 4);
     A((void**)&s->adam_m, NPARAM * 4); A((void**)&s->adam_v, NPARAM * 4);
     A((void**)&s->pk, 4 * 9216 * 2); A((void**)&s->w1r, 288 * 4); A((void**)&s->w4r, 288 * 4);
+    A((void**)&s->thin, (512 + 4608) * 2);
     for (auto** p : {&s->z1, &s->h1, &s->z2, &s->h2, &s->z3, &s->h3, &s->dz, &s->dz2}) A((void**)p, N * CH * 2);
     A((void**)&s->o, N * 4); A((void**)&s->dO, N * 4);
     A((void**)&s->sums, sizeof(double) * (2 * L4_MAXBLK + 1) * batch_max);  // partials + corrections
@@ -1023,13 +1358,20 @@ int phix_surrogate_destroy(phix_surrogate_t* s) {
     for (void* p : {(void*)s->params, (void*)s->grads, (void*)s->adam_m, (void*)s->adam_v, (void*)s->pk,
                     (void*)s->w1r, (void*)s->w4r, (void*)s->z1, (void*)s->h1, (void*)s->z2, (void*)s->h2,
                     (void*)s->z3, (void*)s->h3, (void*)s->dz, (void*)s->dz2, (void*)s->o, (void*)s->dO,
-                    (void*)s->sums, (void*)s->partial, (void*)s->lpart, (void*)s->err, (void*)s->thin_out})
+                    (void*)s->sums, (void*)s->partial, (void*)s->lpart, (void*)s->err, (void*)s->thin_out,
+                    (void*)s->thin})
         if (p) cudaFree(p);
     delete s;
     return PHIX_OK;
 }
 
 int phix_surrogate_nparams(void) { return NPARAM; }
+
+int phix_surrogate_set_fused(phix_surrogate_t* s, int on) {
+    if (!s) { set_error("surrogate_set_fused: NULL surrogate"); return PHIX_ERR_ARG; }
+    s->fused = on != 0;
+    return PHIX_OK;
+}
 
 int phix_surrogate_set_params(phix_surrogate_t* s, const float* host_params) {
     if (!s || !host_params) { set_error("set_params: NULL"); return PHIX_ERR_ARG; }

@@ -101,3 +101,42 @@ def test_trained_surrogate_beats_no_network_baseline(cuda):
         assert r["rel_l2"] < r["baseline_rel_l2"]
     last = rows[-1]
     assert last["rel_l2"] < 6e-2 and last["rel_l2"] < 0.2 * last["baseline_rel_l2"], last
+
+
+@pytest.mark.parametrize("shape", [(12, 256, 2), (512, 512, 1), (37, 384, 3)])
+def test_fused_step_matches_layer_kernels(cuda, shape):
+    """The fused step kernel (all four layers as UMMAs, activations kept in
+    shared memory) against the per-layer kernels.  The two differ only in the
+    FP32 summation order (the fused kernel sums the three x-taps of each
+    layer outside the tensor core); that moves an occasional BF16 activation
+    across a rounding boundary (one BF16 step is 2^-8 relative), so the
+    updates agree to 5e-4 in rel-L2 and to 1e-2 of their size at any pixel.
+    Both conserve the mean mass exactly."""
+    from phix_b200 import surrogate as S
+    h, w, nb = shape
+    trained = (h, w) == (512, 512)
+    p = S.load_params() if trained else px.surrogate_params_to_flat(setup(9)[0])
+    rng = np.random.default_rng(11)
+    c = rng.uniform(0.35, 0.65, size=(nb, h, w)) + 0.01 * rng.standard_normal((nb, h, w))
+    if trained:
+        sg = px.Surrogate(h, w, nb, S.IN_SHIFT, S.IN_SCALE, S.OUT_SCALE)
+    else:
+        sg = px.Surrogate(h, w, nb, SHIFT, SCALE, OSCALE)
+    sg.set_params(p)
+    dc = torch.from_numpy(c).cuda()
+    outs = []
+    for fused in (False, True):
+        sg.set_fused(fused)
+        out = torch.empty_like(dc)
+        sg.step(dc, out)
+        torch.cuda.synchronize()
+        outs.append(out.cpu().numpy())
+    sg.close()
+    ref, got = outs
+    upd = np.abs(ref - c).max()
+    r = rel(got - c, ref - c)
+    print(shape, "rel-L2 of the update", r, "max |fused - layers|", np.abs(got - ref).max(), "update", upd)
+    assert r <= 5e-4
+    assert np.abs(got - ref).max() <= 1e-2 * upd
+    for b in range(nb):
+        assert abs(got[b].sum() - c[b].sum()) <= 1e-12 * abs(c[b].sum())
