@@ -653,9 +653,10 @@ __global__ void __launch_bounds__(256) apply_correction(double* __restrict__ c_o
 // (M128 N16 K16, output channel 0 of 16; the other 15 weight rows are zero).
 // The CUDA cores build the im2col tiles and run the epilogues.
 //
-// Ticks.  At tick t one thread issues this tick's UMMAs into TMEM
-// accumulator set t & 1 while all threads run the epilogues of tick t - 1's
-// UMMAs (set (t - 1) & 1), so the tensor cores and the epilogues overlap:
+// Ticks.  At tick t three warps issue this tick's UMMAs into TMEM accumulator
+// set t & 1 (one thread per accumulator chain) while 16 warps run the
+// epilogues of tick t - 1's UMMAs (set (t - 1) & 1), so the tensor cores and
+// the epilogues overlap:
 //   tick t UMMAs:      layer 1 -> row Y-4+t, layer 2 -> Y-7+t,
 //                      layer 3 -> Y-10+t, layer 4 -> Y-13+t;
 //   tick t epilogues:  the rows of tick t - 1;  im2col of row Y-3+t.
@@ -673,7 +674,7 @@ __global__ void __launch_bounds__(256) apply_correction(double* __restrict__ c_o
 // finish_projection applies the correction.
 constexpr int FW = 122;                      // output pixels per window
 constexpr int F_EW = 16;                     // epilogue warps: TMEM lane quadrant (w % 4), 8-channel chunk (w / 4)
-constexpr int F_NT = 32 * (F_EW + 1);        // + one warp that issues the UMMAs
+constexpr int F_NT = 32 * (F_EW + 3);        // + three warps that issue the UMMAs (layers 1-2, 3, 4)
 constexpr int IM_B = 2 * TILE * 16;          // 4096: im2col tile [k chunk][128 px][8] bf16 (taps 0-7 | 8, 0..)
 constexpr int W1PK_B = 2 * 32 * 16;          // 1024: layer-1 weights [k chunk][32 n][8]
 constexpr int W4PK_B = 9 * 2 * 2 * 16 * 16;  // 9216: layer-4 weights [tap][k16][chunk][16 n][8]
@@ -799,11 +800,15 @@ __global__ void __launch_bounds__(F_NT, 1) step_fused_tc(const FusedArgs a) {
     for (int t = 0; t < nticks; ++t) {
         const int set = t & 1;
         const uint32_t tset = tmem + (uint32_t)(128 * set);
-        if (warp == F_EW && lane == 0) {
+        if (warp >= F_EW && lane == 0) {
             // Shared-memory descriptors are linear in the address (bits 0-13 =
             // address / 16, no carry below 256 KB), so each UMMA's descriptors
-            // are a per-row base plus a compile-time offset.
-            if (live(0, t)) {
+            // are a per-row base plus a compile-time offset.  One thread per
+            // accumulator chain issues (layers 1-2, layer 3, layer 4), each
+            // committing its own barriers: a single issuing thread is bound by
+            // the issue latency of its UMMAs.
+            const int iw = warp - F_EW;
+            if (iw == 0 && live(0, t)) {
                 const uint64_t ad = tc::sdesc(sa + F_IM + ((t - 1) % F_IMS) * IM_B, TILE * 16, 128);
                 tc::umma_bf16(tset, ad, w1d, id32, 0);
                 tc::umma_commit(bar + 0 * 2 + set);
@@ -822,9 +827,9 @@ __global__ void __launch_bounds__(F_NT, 1) step_fused_tc(const FusedArgs a) {
                         tc::umma_bf16(tset + col, ad, bd, id, (tap | kk) != 0);
                     }
             };
-            if (live(1, t)) { conv(F_H1, w2d, row_of(1, t), 32, id32, 1024); tc::umma_commit(bar + 1 * 2 + set); }
-            if (live(2, t)) { conv(F_H2, w3d, row_of(2, t), 64, id32, 1024); tc::umma_commit(bar + 2 * 2 + set); }
-            if (live(3, t)) { conv(F_H3, w4d, row_of(3, t), 96, id16, 512); tc::umma_commit(bar + 3 * 2 + set); }
+            if (iw == 0 && live(1, t)) { conv(F_H1, w2d, row_of(1, t), 32, id32, 1024); tc::umma_commit(bar + 1 * 2 + set); }
+            if (iw == 1 && live(2, t)) { conv(F_H2, w3d, row_of(2, t), 64, id32, 1024); tc::umma_commit(bar + 2 * 2 + set); }
+            if (iw == 2 && live(3, t)) { conv(F_H3, w4d, row_of(3, t), 96, id16, 512); tc::umma_commit(bar + 3 * 2 + set); }
         }
         for (int k = 0; k < 4; ++k)
             if (live(k, t)) pending |= 1u << (2 * k + set);
