@@ -389,58 +389,115 @@ struct March3D {
     }
 };
 
+// The boundary mapping of one in-plane coordinate, resolved once per CTA:
+// the mapped coordinate q, or (q == MAP_CONST_Q) the constant the mapping
+// gives (map_axis / mu_axis semantics).
+constexpr int MAP_CONST_Q = -0x40000000;
+
 template <typename T, class Pol, int MODE, int TX, int TY, int RZ, int NT>
 __global__ void __launch_bounds__(NT) stage_march3d(const StageArgs<T> A, const Pol pol) {
     using G = March3D<T, Pol, TX, TY>;
-    constexpr int NF = G::NF, H = G::H, WX = G::WX, WP = G::WP, MX = G::MX, MP = G::MP;
+    constexpr int NF = G::NF, H = G::H, WX = G::WX, WY = G::WY, WP = G::WP, MX = G::MX, MY = G::MY, MP = G::MP;
     constexpr int NYR = G::NYR, NMR = G::NMR;
     constexpr bool MU = Pol::MU;
+    constexpr int YC = (WP + NT - 1) / NT, MC = (MP + NT - 1) / NT, KC = (TX * TY + NT - 1) / NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* ysb = reinterpret_cast<T*>(smem_raw);   // [NF][NYR][WP]
     T* msb = ysb + (size_t)NF * NYR * WP;      // [NMR][MP]
+    // per-axis maps: y planes (global x, s1 * y) and mu planes (tile offsets)
+    __shared__ int yqx[WX], yqy[WY], mqx[MX], mqy[MY];
+    __shared__ double ycx[WX], ycy[WY], mcx[MX], mcy[MY];
 
-    const int n0 = A.L.n[0], n1 = A.L.n[1], n2 = A.L.n[2];
+    const Layout& L = A.L;
+    const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * RZ;
     const int z1 = min(z0 + RZ, n2);
-    const bool in_xy = x0 - H >= 0 && x0 + TX + H <= n0 && y0 - H >= 0 && y0 + TY + H <= n1;
+
+    for (int i = threadIdx.x; i < WX + WY + MX + MY; i += NT) {
+        int q;
+        double cv = 0.0;
+        if (i < WX) {
+            const bool c = map_axis(x0 - H + i, n0, L.bc[0], L.bc[1], L.bcv[0], L.bcv[1], L.ghost, &q, &cv) == MAP_CONST;
+            yqx[i] = c ? MAP_CONST_Q : q;
+            ycx[i] = cv;
+        } else if (i < WX + WY) {
+            const int k = i - WX;
+            const bool c = map_axis(y0 - H + k, n1, L.bc[2], L.bc[3], L.bcv[2], L.bcv[3], L.ghost, &q, &cv) == MAP_CONST;
+            yqy[k] = c ? MAP_CONST_Q : L.s[1] * q;
+            ycy[k] = cv;
+        } else if (i < WX + WY + MX) {
+            const int k = i - WX - WY;
+            const bool c = mu_axis(x0 - 1 + k, n0, L.bc[0], L.bc[1], L.bcv[0], L.bcv[1], &q, &cv) == MAP_CONST;
+            mqx[k] = c ? MAP_CONST_Q : q - x0 + H;
+            mcx[k] = cv;
+        } else {
+            const int k = i - WX - WY - MX;
+            const bool c = mu_axis(y0 - 1 + k, n1, L.bc[2], L.bc[3], L.bcv[2], L.bcv[3], &q, &cv) == MAP_CONST;
+            mqy[k] = c ? MAP_CONST_Q : (q - y0 + H) * WX;
+            mcy[k] = cv;
+        }
+    }
+    __syncthreads();
 
     auto yslot = [&](int f, int z) -> T* { return ysb + ((size_t)f * NYR + (unsigned)(z + 8 * NYR) % NYR) * WP; };
     auto mslot = [&](int z) -> T* { return msb + (size_t)((unsigned)(z + 8 * NMR) % NMR) * MP; };
 
+    // plane z of the stage state y = u (+ a kin), tile + H: map3's order of
+    // constants (x, then y, then z)
     auto form_y = [&](int z) {
-        const bool interior = in_xy && z >= 0 && z < n2;
-        for (int i = threadIdx.x; i < WP; i += NT) {
-            const int lx = i % WX, ly = i / WX;
+        int qz;
+        double zc = 0.0;
+        const bool zcst = map_axis(z, n2, L.bc[4], L.bc[5], L.bcv[4], L.bcv[5], L.ghost, &qz, &zc) == MAP_CONST;
+        const int zoff = L.origin + L.s[2] * qz;
+        T* dst[NF];
 #pragma unroll
-            for (int f = 0; f < NF; ++f)
-                yslot(f, z)[i] = load_y<T, 3>(A, f, x0 - H + lx, y0 - H + ly, z, interior);
+        for (int f = 0; f < NF; ++f) dst[f] = yslot(f, z);
+#pragma unroll
+        for (int c = 0; c < YC; ++c) {
+            const int i = threadIdx.x + c * NT;
+            if (c + 1 < YC || i < WP) {
+                const int lx = i % WX, ly = i / WX;
+                const int qx = yqx[lx], qy = yqy[ly];
+                const bool cst = qx == MAP_CONST_Q || qy == MAP_CONST_Q || zcst;
+                const double cv = qx == MAP_CONST_Q ? ycx[lx] : qy == MAP_CONST_Q ? ycy[ly] : zc;
+                const int idx = zoff + qx + qy;
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    T v;
+                    if (cst) {
+                        v = (T)cv;
+                    } else {
+                        v = __ldg(A.u[f] + idx);
+                        if (A.kin[f] != nullptr) v = rfma(A.a, __ldg(A.kin[f] + idx), v);
+                    }
+                    dst[f][i] = v;
+                }
+            }
         }
     };
-    // mu at plane z (possibly outside the domain along z).
+    // mu at plane z: mu_axis's order of constants (z, then x, then y)
     auto form_mu = [&](int z) {
         int qz = z;
-        double zval = 0.0;
-        const bool zconst = mu_axis(z, n2, A.L.bc[4], A.L.bc[5], A.L.bcv[4], A.L.bcv[5], &qz, &zval) == MAP_CONST;
+        double zc = 0.0;
+        const bool zcst = mu_axis(z, n2, L.bc[4], L.bc[5], L.bcv[4], L.bcv[5], &qz, &zc) == MAP_CONST;
         T* dst = mslot(z);
-        for (int i = threadIdx.x; i < MP; i += NT) {
-            const int lx = i % MX, ly = i / MX;
-            const int px = x0 - 1 + lx, py = y0 - 1 + ly;
-            int qx = px, qy = py;
-            double cval = zval;
-            bool cst = zconst;
-            if (!cst && !in_xy) {
-                cst = mu_axis(px, n0, A.L.bc[0], A.L.bc[1], A.L.bcv[0], A.L.bcv[1], &qx, &cval) == MAP_CONST;
-                if (!cst) cst = mu_axis(py, n1, A.L.bc[2], A.L.bc[3], A.L.bcv[2], A.L.bcv[3], &qy, &cval) == MAP_CONST;
+        const T* yc0 = yslot(0, qz);
+        const T* ym0 = yslot(0, qz - 1);
+        const T* yp0 = yslot(0, qz + 1);
+        const T* yc1 = yslot(NF - 1, qz);
+#pragma unroll
+        for (int c = 0; c < MC; ++c) {
+            const int i = threadIdx.x + c * NT;
+            if (c + 1 < MC || i < MP) {
+                const int lx = i % MX, ly = i / MX;
+                const int ox = mqx[lx], oy = mqy[ly];
+                T v;
+                if (zcst) v = (T)zc;
+                else if (ox == MAP_CONST_Q) v = (T)mcx[lx];
+                else if (oy == MAP_CONST_Q) v = (T)mcy[ly];
+                else v = compute_mu<T, Pol, 3, WX>(A, pol, yc0, ym0, yp0, yc1, ox + oy);
+                dst[i] = v;
             }
-            T v;
-            if (cst) {
-                v = (T)cval;
-            } else {
-                const int off = (qx - x0 + H) + (qy - y0 + H) * WX;
-                v = compute_mu<T, Pol, 3, WX>(A, pol, yslot(0, qz), yslot(0, qz - 1), yslot(0, qz + 1),
-                                               yslot(NF - 1, qz), off);
-            }
-            dst[i] = v;
         }
     };
 
@@ -465,21 +522,30 @@ __global__ void __launch_bounds__(NT) stage_march3d(const StageArgs<T> A, const 
         const T* y1c = yslot(NF - 1, z);
         const T* y1m = yslot(NF - 1, z - 1);
         const T* y1p = yslot(NF - 1, z + 1);
-        for (int i = threadIdx.x; i < TX * TY; i += NT) {
-            const int lx = i % TX, ly = i / TX;
-            const int px = x0 + lx, py = y0 + ly;
-            if (px >= n0 || py >= n1) continue;
-            const int yoff = (lx + H) + (ly + H) * WX;
-            const int moff = (lx + 1) + (ly + 1) * MX;
-            T k[2];
-            compute_rhs<T, Pol, 3, WX, MX>(A, pol, mslot(z), mslot(z - 1), mslot(z + 1), moff, y0c, y0m, y0p, y1c,
-                                            y1m, y1p, yoff, k);
-            const int idx = A.L.origin + px + A.L.s[1] * py + A.L.s[2] * z;
+        const T* mc = mslot(z);
+        const T* mm = mslot(z - 1);
+        const T* mp = mslot(z + 1);
+        const int zidx = L.origin + L.s[2] * z;
 #pragma unroll
-            for (int f = 0; f < NF; ++f) emit<T, MODE>(A, f, idx, k[f]);
+        for (int c = 0; c < KC; ++c) {
+            const int i = threadIdx.x + c * NT;
+            if (c + 1 < KC || i < TX * TY) {
+                const int lx = i % TX, ly = i / TX;
+                const int px = x0 + lx, py = y0 + ly;
+                if (px < n0 && py < n1) {
+                    const int yoff = (lx + H) + (ly + H) * WX;
+                    const int moff = (lx + 1) + (ly + 1) * MX;
+                    T k[2];
+                    compute_rhs<T, Pol, 3, WX, MX>(A, pol, mc, mm, mp, moff, y0c, y0m, y0p, y1c, y1m, y1p, yoff, k);
+                    const int idx = zidx + px + L.s[1] * py;
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) emit<T, MODE>(A, f, idx, k[f]);
+                }
+            }
         }
         if (MODE != MODE_K) {
-            const int gl = A.L.ghost;
+            const bool in_xy = x0 - H >= 0 && x0 + TX + H <= n0 && y0 - H >= 0 && y0 + TY + H <= n1;
+            const int gl = L.ghost;
             if (!in_xy) {
                 if (x0 == 0 || x0 + TX >= n0)
                     for (int i = threadIdx.x; i < TY * gl; i += NT) {
