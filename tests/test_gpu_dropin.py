@@ -7,6 +7,12 @@ write the same fields bit for bit.
     a .field file every 500 steps (the fused single-equation Solver path).
   * develop/fieldOperation/test_fieldops.cu: the reference's own known-answer
     checks of pw / field arithmetic / composite products (tolerance 1e-12).
+  * applications/solvers/Cahn-Hillard_double-well/2D: the CH application
+    (config file, BC factory, multi-step STEADY/TRANSIENT Euler Solver,
+    OutputWriter in all three formats).  Ours runs twice: with the default
+    asynchronous OutputWriter and with "async": false (the reference's
+    synchronous order); those two runs must write the same bytes, and both
+    must match the reference's files to 1e-12.
 
 The binaries are built where the reference tree exists; without them the
 tests skip.
@@ -70,3 +76,80 @@ def test_fieldops_known_answers(cuda, tmp_path):
     assert rc_o == 0 and "ALL TESTS PASSED" in out_o, out_o[-3000:]
     verdicts = lambda s: [l.strip() for l in s.splitlines() if "[PASS]" in l or "[FAIL]" in l]
     assert verdicts(out_o) == verdicts(out_r)
+
+
+CH_SETTINGS = """{{
+    // written by tests/test_gpu_dropin.py
+    "mesh": {{"nx": {nx}, "ny": {ny}, "dx": 1.0, "dy": 1.0, "x0": 0.0, "y0": 0.0}},
+    "initialize": {{"start_from": "initial_field", "dt": 0.01, "nSteps": {nsteps}}},
+    "boundary_conditions": {{"x_min": "Periodic", "x_max": "Periodic", "y_min": "NoFlux", "y_max": "NoFlux"}},
+    "constants": {{"M": 1.0, "kappa": 0.5, "rho": 1.0, "ca": 0.0, "cb": 1.0}},
+    "output": {{"print_interval": {every}, "write_interval": {every}, "format": "ALL"{extra}}}
+}}
+"""
+
+
+def _write_field(path, name, a):
+    """A 2-D .field file in the reference's binary format (physical cells,
+    little-endian FP64, x fastest)."""
+    ny, nx = a.shape
+    hdr = f"# PhiX ScalarField\nname    {name}\nnx {nx}  ny {ny}  nz 1\nghost   1\n---\n".encode()
+    with open(path, "wb") as f:
+        f.write(hdr + np.ascontiguousarray(a, dtype="<f8").tobytes())
+
+
+def _numbers_close(a, b, tol):
+    """Two text files with the same lines, numbers allowed to differ by tol."""
+    la, lb = a.decode().splitlines(), b.decode().splitlines()
+    if len(la) != len(lb):
+        return False
+    worst = 0.0
+    for x, y in zip(la, lb):
+        if x == y:
+            continue
+        tx, ty = x.split(), y.split()
+        if len(tx) != len(ty):
+            return False
+        for u, v in zip(tx, ty):
+            if u != v:
+                worst = max(worst, abs(float(u) - float(v)))
+    return worst <= tol
+
+
+def test_ch_app_output_identical(cuda, tmp_path):
+    exes = {"ref": _bin("chapp_ref"), "async": _bin("chapp_phix"), "sync": _bin("chapp_phix")}
+    nx, ny, nsteps, every = 160, 96, 1000, 100
+    rng = np.random.default_rng(4)
+    c0 = 0.5 + rng.uniform(-0.01, 0.01, size=(ny, nx))
+    out, files = {}, {}
+    for tag, exe in exes.items():
+        d = tmp_path / tag
+        (d / "settings" / "initial_field").mkdir(parents=True)
+        extra = ', "async": false' if tag == "sync" else ""
+        (d / "settings" / "settings.jsonc").write_text(
+            CH_SETTINGS.format(nx=nx, ny=ny, nsteps=nsteps, every=every, extra=extra))
+        _write_field(d / "settings" / "initial_field" / "c.field", "c", c0)
+        _write_field(d / "settings" / "initial_field" / "mu.field", "mu", np.zeros_like(c0))
+        rc, text = _run(exe, d)
+        assert rc == 0, text[-2000:]
+        out[tag] = [l for l in text.splitlines() if "written:" in l]
+        files[tag] = {n: (d / "output" / n).read_bytes() for n in sorted(os.listdir(d / "output"))}
+    names = sorted(files["ref"])
+    assert len(names) == 3 * (nsteps // every + 1)
+    assert sorted(files["async"]) == sorted(files["sync"]) == names
+    assert out["async"] == out["sync"] == out["ref"] and len(out["ref"]) == nsteps // every + 1
+    for n in names:
+        assert files["async"][n] == files["sync"][n], f"{n}: async and sync output differ"
+    worst = 0.0
+    for n in names:
+        a, b = files["ref"][n], files["async"][n]
+        if n.endswith(".field"):
+            cut = a.index(b"---\n") + 4
+            assert a[:cut] == b[:cut], n
+            da, db = np.frombuffer(a[cut:], "<f8"), np.frombuffer(b[cut:], "<f8")
+            assert da.shape == db.shape == (nx * ny,)
+            worst = max(worst, float(np.abs(da - db).max()))
+        else:
+            assert _numbers_close(a, b, 1e-12), f"{n}: text differs beyond 1e-12"
+    assert worst <= 1e-12, worst
+    print(f"CH app: {len(names)} files, async == sync byte for byte, max-abs vs reference {worst:.1e}")
