@@ -11,7 +11,8 @@ One bench "step" = one output interval: STEPS_PER_INTERVAL RK4 time steps of
 the whole field, replayed from a CUDA graph (the library's default launch
 shape: one launch per stage in FP64, one per time step in FP32; --launch
 overrides it).  --workload selects the other configurations (ac2d, chac3d,
-batch), reported with the same keys.  L2 is flushed (256 MiB write) between timed steps, outside the timed
+batch, and ch2d_ms: the CH application's multi-step form), reported with
+the same keys.  L2 is flushed (256 MiB write) between timed steps, outside the timed
 events.  `value` = cell-updates/s = cells x time steps / device time.
 `e2e` runs the same interval through the C ABI with pinned HOST buffers
 (phix_stepper_run_host: H2D, advance, D2H, synchronise) inside the timed
@@ -110,7 +111,11 @@ def reference_cpu_rate(fields, g, phys, prm, scheme, dt, nsteps):
                 bc=tuple(g.bc_type), bc_val=tuple(g.bc_val))
     work = [f.copy() for f in fields]
     t0 = time.perf_counter()
-    ref.advance(work, phys, prm, scheme, dt, nsteps, grid, use_gpu=False)
+    from phix_b200 import MULTISTEP  # a constant: the CUDA library is not loaded
+    if scheme == MULTISTEP:  # c and mu
+        ref.advance_ch_multistep(work[0], work[1], prm, dt, nsteps, grid, use_gpu=False)
+    else:
+        ref.advance(work, phys, prm, scheme, dt, nsteps, grid, use_gpu=False)
     el = time.perf_counter() - t0
     cells = g.n[0] * g.n[1] * g.n[2]
     return cells * nsteps / el, el
@@ -123,6 +128,8 @@ def reference_cpu_rate(fields, g, phys, prm, scheme, dt, nsteps):
 WORKLOADS = {
     "ch2d": ("CH 1024^2 periodic, single-equation RK4, dt=0.005 (spinodal decomposition)",
              "synthetic: c0 = 0.5 + U[-0.01,0.01], numpy default_rng(1)"),
+    "ch2d_ms": ("CH 1024^2 periodic, multi-step Euler (mu STEADY, c TRANSIENT: the CH application's form), dt=0.005",
+                "synthetic: c0 = 0.5 + U[-0.01,0.01], numpy default_rng(1); mu0 = 0"),
     "ac2d": ("AC 128^2 periodic, Euler, dt=0.01, L=kappa=1 (quickstart form)",
              "synthetic: phi0 = U[-0.05,0.05], numpy default_rng(0)"),
     "chac3d": ("CH+AC 3-D 256^3, zero-flux x, periodic y/z, coupled RK4, dt=0.002",
@@ -149,6 +156,8 @@ FIRST_PAIR_TILE = 6
 def dominant_kernel(px, g, phys, scheme, lps, fused, tile):
     """Name of the kernel that takes the time step (the key of TRAFFIC)."""
     periodic_ch = phys == px.PHYS_CH and g.dim == 2 and all(g.bc_type[i] == px.BC_PERIODIC for i in range(4))
+    if scheme == px.MULTISTEP:
+        return "step_pair_ms" if fused else "stage_box"
     if lps == 1 and scheme == px.RK4 and fused:
         return "step_pair" if (tile >= FIRST_PAIR_TILE or (tile == -1 and periodic_ch)) else "step_box"
     return "stage_box" if tile == -1 else "stage_col"
@@ -162,6 +171,9 @@ class StepperRun:
         if args.workload == "ch2d":
             g, phys, prm, scheme, dt, _, fields = workloads.ch2d(n=args.n)
             self.K = STEPS_PER_INTERVAL
+        elif args.workload == "ch2d_ms":
+            g, phys, prm, scheme, dt, _, fields = workloads.ch2d_ms(n=args.n)
+            self.K = STEPS_PER_INTERVAL
         elif args.workload == "ac2d":
             g, phys, prm, scheme, dt, _, fields = workloads.ac2d()
             self.K = 100
@@ -171,9 +183,11 @@ class StepperRun:
         self.prec = px.F64 if args.dtype == "f64" else px.F32
         w = 8 if self.prec == px.F64 else 4
         self.nf = len(fields)
-        self.cells = g.n[0] * g.n[1] * g.n[2] * self.nf  # field-cell updates per time step
-        # RK4: R u,W k1 | R u,k1 W k2 | R u,k2 W k3 | R u,k1,k2,k3 W u' = 13w; Euler: R u, W u' = 2w
-        self.alg_bytes = (13 if scheme == px.RK4 else 2) * w * self.cells
+        # field-cell updates per time step (multi-step: c advances, mu is formed)
+        self.cells = g.n[0] * g.n[1] * g.n[2] * (1 if scheme == px.MULTISTEP else self.nf)
+        # RK4: R u,W k1 | R u,k1 W k2 | R u,k2 W k3 | R u,k1,k2,k3 W u' = 13w; Euler: R u, W u' = 2w;
+        # multi-step: R c, W c', W mu = 3w
+        self.alg_bytes = {px.RK4: 13, px.MULTISTEP: 3}.get(scheme, 2) * w * self.cells
         self.fields, self.g, self.phys, self.prm, self.scheme, self.dt = fields, g, phys, prm, scheme, dt
         self.st = px.Stepper(phys, scheme, self.prec, prm, dt, g)
         if args.launch != "auto":
@@ -499,11 +513,11 @@ def bench_surrogate(args):
     fd = S.time_speed(p, sur_steps=SUR_K)
     flops = 2 * 9 * (32 + 32 * 32 + 32 * 32 + 32) * n * n  # per surrogate step
     achieved = flops * SUR_K / (ms_per_step / 1e3) / 1e12
-    peak = None
+    peak, peak_kind = 1590.0, "fallback"  # dense BF16 TFLOP/s measured earlier on this pool's B200s
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
         with open(pk) as f:
-            peak = float(json.load(f)["bf16_tflops"])
+            peak, peak_kind = float(json.load(f)["bf16_tflops"]), "measured"
     line = {
         "metric": "surrogate vs FD sim-time/s (CH 512^2, one surrogate step = 50 FD steps)",
         "value": value, "unit": "simulated time units/s", "n_gpus": 1, "steps": args.steps,
@@ -520,7 +534,7 @@ def bench_surrogate(args):
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None, "traffic": None,
                      "note": "9.97 GFLOP per surrogate step (2*9*(32+1024+1024+32) per pixel) over the "
-                             "CUDA-event time of the whole step (all kernels); peak bf16_tflops measured"},
+                             f"CUDA-event time of the whole step (all kernels); peak bf16_tflops {peak_kind}"},
         "e2e": {"value": sim_per_step / (e2e_ms / 1e3), "unit": "simulated time units/s",
                 "h2d_bytes_per_step": h_in.numel() * 8, "d2h_bytes_per_step": h_out.numel() * 8},
         "gpu_launches": launches,

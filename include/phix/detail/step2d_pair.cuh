@@ -168,6 +168,59 @@ __device__ __forceinline__ void pair_k_pass(const StageArgs<T>& S, const T* __re
     });
 }
 
+// u on the tile + E (periodic images of out-of-domain cells) into U (row
+// pitch P, R rows): this thread's pair column on rows rp, rp + NRP, ...; all
+// loads are issued before the first shared-memory store.  `inside`: the tile
+// + E lies in the grid, so no image mapping is needed.
+template <typename T, int E, int P, int R, int NRP>
+__device__ __forceinline__ void pair_load_tile(const StageArgs<T>& S, T* __restrict__ U, int x0, int y0, int pc,
+                                               int rp, bool inside) {
+    using V = typename PairOf<T>::V;
+    const Layout& L = S.L;
+    constexpr int NLD = (R + NRP - 1) / NRP;
+    V v[NLD];
+    const int px = x0 - E + 2 * pc;
+#pragma unroll
+    for (int i = 0; i < NLD; ++i) {
+        const int ly = rp + i * NRP, py = y0 - E + ly;
+        if (ly < R) {
+            if (inside) {
+                const T* g = S.u[0] + L.origin + px + L.s[1] * py;
+                v[i] = V{__ldg(g), __ldg(g + 1)};
+            } else {
+                int i0, i1;
+                double cval;
+                map3<2>(L, px, py, 0, &i0, &cval);  // periodic only: never MAP_CONST
+                map3<2>(L, px + 1, py, 0, &i1, &cval);
+                v[i] = V{__ldg(S.u[0] + i0), __ldg(S.u[0] + i1)};
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NLD; ++i) {
+        const int ly = rp + i * NRP;
+        if (ly < R) p_st(U + ly * P + 2 * pc, v[i]);
+    }
+}
+
+// The low parts of the compensated state at this thread's cells of the tile
+// pass (region R0: rows fr0 + j, pair at x = gx), zero where there are none.
+template <typename T, class R0, int E>
+__device__ __forceinline__ void pair_lo_prefetch(const StageArgs<T>& S, typename PairOf<T>::V* lo_pf, int y0, int fr0,
+                                                 int gx, bool fcol, bool x1, int rp) {
+    const Layout& L = S.L;
+#pragma unroll
+    for (int j = 0; j <= R0::Q; ++j) {
+        lo_pf[j] = p_splat((T)0);
+        const int py = y0 + fr0 + j - E;
+        if (S.ulo[0] && fcol && (j < R0::Q || rp < R0::REM) && py < L.n[1] && gx < L.n[0]) {
+            const T* g = S.ulo[0] + L.origin + gx + L.s[1] * py;
+            lo_pf[j].x = __ldg(g);
+            if (x1) lo_pf[j].y = __ldg(g + 1);
+        }
+    }
+}
+
 template <typename T, int TX, int TY, int NRP>
 __device__ __forceinline__ void step_pair_tile(const StepArgs<T>& A, T* __restrict__ sm, int x0, int y0) {
     using G = StepPair<T, TX, TY, NRP>;
@@ -182,36 +235,8 @@ __device__ __forceinline__ void step_pair_tile(const StepArgs<T>& A, T* __restri
     const int n0 = L.n[0], n1 = L.n[1];
     const int pc = threadIdx.x % NC, rp = threadIdx.x / NC;
 
-    // u on the tile + E (periodic images of out-of-domain cells): this
-    // thread's pair column on rows rp, rp + NRP, ...; all loads are issued
-    // before the first shared-memory store
     const bool inside = x0 - E >= 0 && x0 + TX + E <= n0 && y0 - E >= 0 && y0 + TY + E <= n1;
-    {
-        constexpr int NLD = (R + NRP - 1) / NRP;
-        V v[NLD];
-        const int px = x0 - E + 2 * pc;
-#pragma unroll
-        for (int i = 0; i < NLD; ++i) {
-            const int ly = rp + i * NRP, py = y0 - E + ly;
-            if (ly < R) {
-                if (inside) {
-                    const T* g = S.u[0] + L.origin + px + L.s[1] * py;
-                    v[i] = V{__ldg(g), __ldg(g + 1)};
-                } else {
-                    int i0, i1;
-                    double cval;
-                    map3<2>(L, px, py, 0, &i0, &cval);  // periodic only: never MAP_CONST
-                    map3<2>(L, px + 1, py, 0, &i1, &cval);
-                    v[i] = V{__ldg(S.u[0] + i0), __ldg(S.u[0] + i1)};
-                }
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < NLD; ++i) {
-            const int ly = rp + i * NRP;
-            if (ly < R) p_st(U + ly * P + 2 * pc, v[i]);
-        }
-    }
+    pair_load_tile<T, E, P, R, NRP>(S, U, x0, y0, pc, rp, inside);
     // the low parts of this thread's cells of the final update, fetched now
     // so that their latency hides behind the four stages
     using R0 = PairRegion<TX, TY, E, NRP, 0>;
@@ -220,18 +245,7 @@ __device__ __forceinline__ void step_pair_tile(const StepArgs<T>& A, T* __restri
     const bool fcol = pc >= R0::PLO && pc < R0::PHI, x1 = gx + 1 < n0;
     constexpr bool LO_STATE = sizeof(T) == 4;  // compensated state: FP32 steppers only
     V lo_pf[LO_STATE ? R0::Q + 1 : 1];
-    if constexpr (LO_STATE) {
-#pragma unroll
-        for (int j = 0; j <= R0::Q; ++j) {
-            lo_pf[j] = p_splat((T)0);
-            const int py = y0 + fr0 + j - E;
-            if (S.ulo[0] && fcol && (j < R0::Q || rp < R0::REM) && py < n1 && gx < n0) {
-                const T* g = S.ulo[0] + L.origin + gx + L.s[1] * py;
-                lo_pf[j].x = __ldg(g);
-                if (x1) lo_pf[j].y = __ldg(g + 1);
-            }
-        }
-    }
+    if constexpr (LO_STATE) pair_lo_prefetch<T, R0, E>(S, lo_pf, y0, fr0, gx, fcol, x1, rp);
     __syncthreads();
 
     // stage 1: y1 = u

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "equation/FusedStage.h"
+#include "phix/detail/step2d_pair_ms.cuh"
 #include "phix_b200.h"
 
 namespace PhiX {
@@ -66,6 +67,17 @@ struct PwKernelsImpl final : fuse::PwKernels {
             pol.c[i] = s.c[i];
         }
         const phix::StageArgs<double>& A = s.A;
+        if constexpr (DIM == 2 && MODE == phix::MODE_MULTISTEP && PAT == fuse::PATTERN_COMPOSITE) {
+            if (phix::step_pair_supported(A.L, 2)) {
+                // the multi-step form on four periodic sides: the pair kernel
+                // (64x16 tiles, 4 row blocks: 22 KB of shared memory, no opt-in)
+                using G = phix::MsPair<double, 64, 16, 4>;
+                dim3 grid((A.L.n[0] + 63) / 64, (A.L.n[1] + 15) / 16, 1);
+                phix::step_pair_ms<double, Pol, 64, 16, 4><<<grid, G::NT, G::smem_bytes(), st>>>(A, pol);
+                count_user_launch();
+                return cudaGetLastError() == cudaSuccess ? PHIX_OK : PHIX_ERR_CUDA;
+            }
+        }
         if (DIM == 3) {
             using G = phix::March3D<double, Pol, 32, 8>;
             dim3 grid((A.L.n[0] + 31) / 32, (A.L.n[1] + 7) / 8, (A.L.n[2] + 15) / 16);

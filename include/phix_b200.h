@@ -160,8 +160,11 @@ int phix_stepper_set_graph(phix_stepper_t* h, int steps_per_graph);
  * stage states in shared memory and recomputes the tile halos; 0: one launch
  * per stage.  Both give the same bits.  Default: 1 for FP32 steppers and for
  * FP64 CH steppers whose four sides are periodic (the pair kernels), else 0
- * (the faster of the two on B200 for each).  No reference counterpart (the
- * reference runs each term and stage as its own kernels). */
+ * (the faster of the two on B200 for each).  PHIX_MULTISTEP steppers on 2-D
+ * grids with four periodic sides: 1 (default) runs the pair-layout step,
+ * 0 the box-tile step; one launch per step either way, same bits.  No
+ * reference counterpart (the reference runs each term and stage as its own
+ * kernels). */
 int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step);
 
 /* Kernel launches one time step takes with the current settings. */
@@ -175,18 +178,22 @@ int phix_stepper_launches_per_step(const phix_stepper_t* h);
  * 6..15 pair tiles (CH with four periodic sides; two cells per thread) of
  * 128x64, 128x32, 128x32, 128x16, 64x32, 64x64, 256x32, 128x28, 64x28, 64x16
  * with 8, 8, 4, 4, 8, 8, 4, 8, 8, 4 row blocks.  Shapes that do not fit in
- * shared memory for the precision are refused when the step runs.  -1 picks
- * by grid (see phix_stepper_autotune for a measured choice).  All give the
- * same bits.  No reference counterpart. */
+ * shared memory for the precision are refused when the step runs.
+ * PHIX_MULTISTEP steppers with the pair-layout step: 0..5 pair tiles of
+ * 128x32, 64x32, 128x16, 64x16, 64x64, 256x16 with 8, 8, 4, 4, 8, 4 row
+ * blocks (threads = (TX/2 + 2) x row blocks).  -1 picks by grid (see
+ * phix_stepper_autotune for a measured choice).  All give the same bits.
+ * No reference counterpart. */
 int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg);
 
 /* The current launch form (1: one launch per RK4 step) and tile shape. */
 int phix_stepper_get_tiles(const phix_stepper_t* h, int* one_launch_per_step, int* tile_cfg);
 
-/* Time every launch form (one launch per stage or per RK4 step) and tile
- * shape this stepper's grid can take, twice on trial_steps steps of its
- * current state, keep the fastest (state saved and restored); *best_ms = ms
- * per step.  RK4 and Euler steppers.  No reference counterpart. */
+/* Time every launch form (one launch per stage or per RK4 step; for
+ * PHIX_MULTISTEP the box-tile and the pair-layout step) and tile shape this
+ * stepper's grid can take, twice on trial_steps steps of its current state,
+ * keep the fastest (state, mu included, saved and restored); *best_ms = ms
+ * per step.  No reference counterpart. */
 int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms);
 
 /* FP64 only: run directly on caller-owned buffers, no copies.  fields[f] is

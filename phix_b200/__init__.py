@@ -241,7 +241,7 @@ class Stepper:
         h = C.c_void_p()
         check(lib().phix_stepper_create(C.byref(h), phys, scheme, precision, _prm(prm), dt, C.byref(g)))
         self.h = h
-        self.nf = NFIELDS[phys]
+        self.nf = 2 if scheme == MULTISTEP else NFIELDS[phys]  # multi-step: c and mu
 
     def close(self):
         if getattr(self, "h", None):

@@ -22,6 +22,7 @@
 #include "phix/detail/stage_col.cuh"
 #include "phix/detail/step2d.cuh"
 #include "phix/detail/step2d_pair.cuh"
+#include "phix/detail/step2d_pair_ms.cuh"
 #include "stepper.h"
 
 namespace phix {
@@ -255,17 +256,65 @@ int pair_dispatch(int i, bool prepare, const StepArgs<T>* A, cudaStream_t s, int
     return PHIX_ERR_ARG;
 }
 
+// tiles of the multi-step pair kernel (CH, four periodic sides): (TX, TY,
+// row blocks); threads = (TX / 2 + 2) x row blocks.
+constexpr int kMsCfgs[][3] = {{128, 32, 8}, {64, 32, 8}, {128, 16, 4}, {64, 16, 4}, {64, 64, 8}, {256, 16, 4}};
+constexpr int kNumMsCfgs = sizeof(kMsCfgs) / sizeof(kMsCfgs[0]);
+
+// prepare: set the shared-memory attribute; occ != nullptr: report resident
+// CTAs per SM; else launch.
+template <typename T, int TX, int TY, int NRP>
+int ms_cfg(bool prepare, const StageArgs<T>* A, cudaStream_t s, int* occ = nullptr) {
+    using G = MsPair<T, TX, TY, NRP>;
+    static_assert(G::smem_bytes() <= kMaxSmem, "multi-step pair tile too large");
+    auto kern = step_pair_ms<T, PolCH, TX, TY, NRP>;
+    if (occ) {
+        PHIX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, G::NT, G::smem_bytes()));
+        return PHIX_OK;
+    }
+    if (prepare) {
+        PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
+        return PHIX_OK;
+    }
+    dim3 grid((A->L.n[0] + TX - 1) / TX, (A->L.n[1] + TY - 1) / TY, 1);
+    kern<<<grid, G::NT, G::smem_bytes(), s>>>(*A, PolCH{});
+    PHIX_LAUNCH_CHECK("step_pair_ms");
+    return PHIX_OK;
+}
+
+template <typename T>
+int ms_dispatch(int i, bool prepare, const StageArgs<T>* A, cudaStream_t s, int* occ = nullptr) {
+    switch (i) {
+#define PHIX_MS_CASE(i) \
+    case i: return ms_cfg<T, kMsCfgs[i][0], kMsCfgs[i][1], kMsCfgs[i][2]>(prepare, A, s, occ);
+        PHIX_MS_CASE(0)
+        PHIX_MS_CASE(1)
+        PHIX_MS_CASE(2)
+        PHIX_MS_CASE(3)
+        PHIX_MS_CASE(4)
+        PHIX_MS_CASE(5)
+#undef PHIX_MS_CASE
+    }
+    set_error("step_pair_ms: bad tile configuration %d", i);
+    return PHIX_ERR_UNSUPPORTED;
+}
+
 template <typename T, int PHYS>
 int prepare_step2d_t() {
     for (int c = 0; c < kNumStepCfgs; ++c) {
         int rc = step_dispatch<T, PHYS>(c, true, nullptr, 0);
         if (rc) return rc;
     }
-    if (PHYS == PHIX_PHYS_CH)
+    if (PHYS == PHIX_PHYS_CH) {
         for (int c = 0; c < kNumPairCfgs; ++c) {
             int rc = pair_dispatch<T>(c, true, nullptr, 0);
             if (rc) return rc;
         }
+        for (int c = 0; c < kNumMsCfgs; ++c) {
+            int rc = ms_dispatch<T>(c, true, nullptr, 0);
+            if (rc) return rc;
+        }
+    }
     return PHIX_OK;
 }
 
@@ -350,6 +399,20 @@ int default_step_cfg(int phys, const Layout& L) {
         if (tiles <= nsm) return 4;
     }
     return 3;
+}
+
+// The multi-step Cahn-Hilliard step in the pair layout (CH, 2-D, four
+// periodic sides); tile < 0 takes the default shape: 64x16 tiles with 4 row
+// blocks, or 128x16 from 4 M cells up (the fastest measured on B200 at
+// 512^2, 1024^2 and 4096^2, FP32 and FP64).
+template <typename T>
+int launch_ms(const StageArgs<T>& A, cudaStream_t s, int tile) {
+    const int cfg = tile >= 0 ? tile : (long long)A.L.n[0] * A.L.n[1] >= (4LL << 20) ? 2 : 3;
+    if (cfg >= kNumMsCfgs) {
+        set_error("step_pair_ms: tile configuration %d out of range", cfg);
+        return PHIX_ERR_UNSUPPORTED;
+    }
+    return ms_dispatch<T>(cfg, false, &A, s);
 }
 
 template <typename T>
@@ -498,6 +561,12 @@ static bool step_fused(const phix_stepper* h) {
     return h->fuse_steps && h->scheme == PHIX_RK4 && h->nf == 1 && step2d_supported(h->L, h->dim);
 }
 
+// Multi-step steppers on 2-D grids with four periodic sides run the pair
+// kernel unless one launch per step is switched off (then stage_box).
+static bool ms_pair(const phix_stepper* h) {
+    return h->fuse_steps && h->scheme == PHIX_MULTISTEP && h->dim == 2 && step_pair_supported(h->L, 2);
+}
+
 static int launches_per_step(const phix_stepper* h) {
     return h->scheme == PHIX_RK4 && !step_fused(h) ? 4 : 1;
 }
@@ -526,7 +595,7 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
         A.mu_out = (T*)h->st[0][1];
         A.dtf = (T)h->dt;
         set_lo(1);
-        rc = launch_stage<T>(h->phys, h->dim, MODE_MULTISTEP, A, s, h->tile);
+        rc = ms_pair(h) ? launch_ms<T>(A, s, h->tile) : launch_stage<T>(h->phys, h->dim, MODE_MULTISTEP, A, s, h->tile);
         if (rc) return rc;
     } else if (h->scheme == PHIX_EULER) {
         for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->st[o][f];
@@ -741,27 +810,30 @@ int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg) {
 
 int phix_stepper_get_tiles(const phix_stepper_t* h, int* one_launch_per_step, int* tile_cfg) {
     if (!h) { set_error("get_tiles: NULL stepper"); return PHIX_ERR_ARG; }
-    if (one_launch_per_step) *one_launch_per_step = step_fused(h) ? 1 : 0;
+    if (one_launch_per_step) *one_launch_per_step = step_fused(h) || ms_pair(h) ? 1 : 0;
     if (tile_cfg) *tile_cfg = h->tile;
     return PHIX_OK;
 }
 
 int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms) {
     if (!h || trial_steps < 1) { set_error("autotune: bad stepper or trial_steps"); return PHIX_ERR_ARG; }
-    if (h->scheme == PHIX_MULTISTEP) {
-        set_error("autotune: RK4 and Euler steppers only");
-        return PHIX_ERR_UNSUPPORTED;
-    }
     // candidates: one launch per stage with every stage tile, and (RK4, one
     // 2-D field with periodic or zero-flux sides) one launch per step with
-    // every step tile
+    // every step tile; multi-step: stage_box, and the pair kernel with every
+    // tile where the grid takes it
     std::vector<std::pair<bool, int>> cand;
-    if (h->dim == 2)
-        for (int t = -1; t < kNumColCfgs; ++t) cand.push_back({false, t});
-    else
+    if (h->scheme == PHIX_MULTISTEP) {
         cand.push_back({false, -1});
-    if (h->scheme == PHIX_RK4 && h->nf == 1 && step2d_supported(h->L, h->dim))
-        for (int t = 0; t < kNumStepCfgs + kNumPairCfgs; ++t) cand.push_back({true, t});
+        if (h->dim == 2 && step_pair_supported(h->L, 2))
+            for (int t = 0; t < kNumMsCfgs; ++t) cand.push_back({true, t});
+    } else {
+        if (h->dim == 2)
+            for (int t = -1; t < kNumColCfgs; ++t) cand.push_back({false, t});
+        else
+            cand.push_back({false, -1});
+        if (h->scheme == PHIX_RK4 && h->nf == 1 && step2d_supported(h->L, h->dim))
+            for (int t = 0; t < kNumStepCfgs + kNumPairCfgs; ++t) cand.push_back({true, t});
+    }
 
     // trials advance the state: save it, and restore it afterwards
     const int cur0 = h->cur;
@@ -771,10 +843,13 @@ int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms) {
     const int parts = h->lo[cur0][0] ? 2 : 1;
     void* save = nullptr;
     PHIX_TRY_CUDA(cudaMalloc(&save, bytes * h->nf * parts));
+    // the multi-step mu field is one buffer (st[0][1]) with no low part
+    const bool ms = h->scheme == PHIX_MULTISTEP;
     auto copy_state = [&](bool to_save) {
         for (int f = 0; f < h->nf; ++f)
             for (int q = 0; q < parts; ++q) {
-                void* buf = q ? h->lo[cur0][f] : h->st[cur0][f];
+                if (ms && f == 1 && q) continue;
+                void* buf = q ? h->lo[cur0][f] : (ms && f == 1 ? h->st[0][1] : h->st[cur0][f]);
                 char* sv = (char*)save + bytes * (f * parts + q);
                 cudaError_t e = to_save ? cudaMemcpy(sv, buf, bytes, cudaMemcpyDeviceToDevice)
                                         : cudaMemcpy(buf, sv, bytes, cudaMemcpyDeviceToDevice);

@@ -9,7 +9,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import (BC_NOFLUX, BC_PERIODIC, EULER, PHYS_AC, PHYS_CH, PHYS_CHAC, RK4, make_grid, stored_shape)
+from . import (BC_NOFLUX, BC_PERIODIC, EULER, MULTISTEP, PHYS_AC, PHYS_CH, PHYS_CHAC, RK4, make_grid, stored_shape)
 
 
 def _stored(g, phys_vals):
@@ -36,6 +36,16 @@ def ch2d(n=1024, seed=1, nsteps=20000, kappa=0.5, M=1.0, c_mean=0.5, noise=0.01,
     rng = np.random.default_rng(seed)
     c = c_mean + rng.uniform(-noise, noise, size=(1, n, n))
     return g, PHYS_CH, [M, kappa, 1.0, 0.0, 1.0], RK4, dt, nsteps, [_stored(g, c)]
+
+
+def ch2d_ms(n=1024, seed=1, nsteps=20000, kappa=0.5, M=1.0, c_mean=0.5, noise=0.01, dt=0.005):
+    """The Cahn-Hilliard application's form (Cahn-Hillard_double-well.cu:
+    mu = f'(c) - kappa lap c as a STEADY field, then dc/dt = M lap mu by
+    Euler), n x n periodic, dx=1, f = c^2(1-c)^2; c0 as in ch2d, mu0 = 0."""
+    g = make_grid((n, n))
+    rng = np.random.default_rng(seed)
+    c = c_mean + rng.uniform(-noise, noise, size=(1, n, n))
+    return g, PHYS_CH, [M, kappa, 1.0, 0.0, 1.0], MULTISTEP, dt, nsteps, [_stored(g, c), _stored(g, np.zeros_like(c))]
 
 
 def chac3d(n=256, seed=2, nsteps=5000):

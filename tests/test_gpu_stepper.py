@@ -267,6 +267,78 @@ def test_multistep_ch_multi_tile_bcs(cuda, oracle, bc):
     assert np.array_equal(got_mu[keep], mu[keep]), _where(got_mu, mu, keep)
 
 
+MS_PAIR_TILES = range(6)  # tile shapes of the multi-step pair kernel (kMsCfgs)
+
+
+@pytest.mark.parametrize("tile", MS_PAIR_TILES)
+@pytest.mark.parametrize("n", [(150, 37), (64, 32), (300, 170)])
+def test_multistep_pair_tiles_match_oracle(cuda, oracle, n, tile):
+    """The multi-step pair kernel (four periodic sides) with every tile shape:
+    c and mu bit for bit against the oracle, partial tiles included."""
+    bcs = (px.BC_PERIODIC,) * 4 + (0, 0)
+    g = px.make_grid(n, (0.9, 1.1), 1, bcs)
+    grid = Grid(n=n, d=(0.9, 1.1), bc=bcs, bc_val=(0,) * 6)
+    rng = np.random.default_rng(31 + tile)
+    c = grid.stored_from_phys(rng.uniform(0.3, 0.7, size=(1, n[1], n[0])))
+    mu = np.zeros_like(c)
+    prm = [1.2, 0.7, 1.5, 0.1, 0.9]
+    st = px.Stepper(px.PHYS_CH, px.MULTISTEP, px.F64, prm, 0.002, g)
+    st.set_tiles(tile)
+    assert st.tiles() == (True, tile) and st.launches_per_step == 1
+    fields = [torch.from_numpy(c.copy()).cuda(), torch.from_numpy(mu.copy()).cuda()]
+    st.load(fields)
+    st.advance(9)
+    st.store(fields)
+    torch.cuda.synchronize()
+    st.close()
+    oracle.advance_ch_multistep(c, mu, prm, 0.002, 9, grid, fma_mode=1)
+    keep = ~corner_mask(grid)
+    got_c, got_mu = fields[0].cpu().numpy(), fields[1].cpu().numpy()
+    assert np.array_equal(got_c[keep], c[keep]), _where(got_c, c, keep)
+    assert np.array_equal(got_mu[keep], mu[keep]), _where(got_mu, mu, keep)
+
+
+@pytest.mark.parametrize("prec", [px.F32, px.F64])
+def test_multistep_pair_matches_stage_box_and_autotune(cuda, prec):
+    """FP32 and FP64: the multi-step pair kernel and stage_box (one launch per
+    step switched off) give the same bits; autotuning restores the loaded c
+    and mu and keeps those bits."""
+    n = (200, 90)
+    bcs = (px.BC_PERIODIC,) * 4 + (0, 0)
+    g = px.make_grid(n, (1.0, 1.0), 1, bcs)
+    grid = Grid(n=n, d=(1.0, 1.0), bc=bcs, bc_val=(0,) * 6)
+    c = grid.stored_from_phys(np.random.default_rng(8).uniform(0.35, 0.65, size=(1, n[1], n[0])))
+    prm = [1.0, 0.5, 1.0, 0.0, 1.0]
+    outs = []
+    for mode in ("box", "pair", "tuned"):
+        st = px.Stepper(px.PHYS_CH, px.MULTISTEP, prec, prm, 0.005, g)
+        fields = [torch.from_numpy(c.copy()).cuda(), torch.from_numpy(np.zeros_like(c)).cuda()]
+        st.load(fields)
+        if mode == "box":
+            st.set_fusion(False)
+            assert st.tiles()[0] is False
+        elif mode == "tuned":
+            before = [torch.empty_like(f) for f in fields]
+            st.advance(3)
+            st.store(before)
+            assert st.autotune(2) > 0
+            after = [torch.empty_like(f) for f in fields]
+            st.store(after)
+            for b, a in zip(before, after):
+                assert torch.equal(b, a)
+        else:
+            assert st.tiles()[0] is True
+        st.advance(12 if mode != "tuned" else 9)
+        st.store(fields)
+        torch.cuda.synchronize()
+        st.close()
+        outs.append([f.cpu().numpy() for f in fields])
+    keep = ~corner_mask(grid)
+    for other in outs[1:]:
+        for f in range(2):
+            assert np.array_equal(other[f][keep], outs[0][f][keep]), _where(other[f], outs[0][f], keep)
+
+
 TILE_CASES = [
     # (phys, n, bcs, bc values)
     (px.PHYS_CH, (300, 70), (px.BC_PERIODIC,) * 4, (0,) * 4),
