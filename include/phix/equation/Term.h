@@ -63,13 +63,20 @@ struct PwKernels {
     virtual int prepare(int dim) const = 0;
 };
 
+struct FlatKernels;  // phix/equation/FlatProgram.h
+
 // What a term computes, for the fused path.
 struct Info {
-    enum Kind { LAP, PW1, LAP_EXPR, OTHER } kind = OTHER;
-    const ScalarField* field = nullptr;         // LAP, PW1
+    enum Kind { LAP, PW1, LAP_EXPR, GRAD, PWN, TIMES_FIELD, TIMES_EXPR, OTHER } kind = OTHER;
+    const ScalarField* field = nullptr;         // LAP, PW1, GRAD, TIMES_FIELD (the field factor)
     std::shared_ptr<const PwKernels> pw;        // PW1
-    std::shared_ptr<const RHSExpr> inner;       // LAP_EXPR
+    std::shared_ptr<const RHSExpr> inner;       // LAP_EXPR, TIMES_FIELD, TIMES_EXPR (first factor)
+    std::shared_ptr<const RHSExpr> inner2;      // TIMES_EXPR (second factor)
     std::vector<BoundaryCondition*> bcs;        // LAP_EXPR
+    int axis = 0;                               // GRAD
+    int nargs = 0;                              // PW1, PWN: the functor's fields
+    const ScalarField* args[3] = {nullptr, nullptr, nullptr};
+    std::shared_ptr<const FlatKernels> flat;    // PW1, PWN: step kernels with this functor
 };
 }  // namespace fuse
 

@@ -9,6 +9,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "equation/FlatProgram.h"
 #include "equation/FusedStage.h"
 #include "phix/detail/step2d_pair_ms.cuh"
 #include "phix_b200.h"
@@ -171,6 +172,9 @@ Term pw(const ScalarField& f, Functor func, double coeff) {
     info->kind = fuse::Info::PW1;
     info->field = pf;
     info->pw = std::make_shared<detail::PwKernelsImpl<Functor>>(func);
+    info->nargs = 1;
+    info->args[0] = pf;
+    info->flat = std::make_shared<fuse::FlatKernelsImpl<Functor, 1>>(func);
     t.fusion = info;
     return t;
 }
@@ -197,6 +201,13 @@ Term pw(const ScalarField& f1, const ScalarField& f2, Functor func, double coeff
                     rhs[idx] += c * func(a[idx], b[idx]);
                 }
     };
+    auto info = std::make_shared<fuse::Info>();
+    info->kind = fuse::Info::PWN;
+    info->nargs = 2;
+    info->args[0] = p1;
+    info->args[1] = p2;
+    info->flat = std::make_shared<fuse::FlatKernelsImpl<Functor, 2>>(func);
+    t.fusion = info;
     return t;
 }
 
@@ -223,6 +234,14 @@ Term pw(const ScalarField& f1, const ScalarField& f2, const ScalarField& f3, Fun
                     rhs[idx] += c * func(a[idx], b[idx], d[idx]);
                 }
     };
+    auto info = std::make_shared<fuse::Info>();
+    info->kind = fuse::Info::PWN;
+    info->nargs = 3;
+    info->args[0] = p1;
+    info->args[1] = p2;
+    info->args[2] = p3;
+    info->flat = std::make_shared<fuse::FlatKernelsImpl<Functor, 3>>(func);
+    t.fusion = info;
     return t;
 }
 

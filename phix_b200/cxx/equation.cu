@@ -215,6 +215,11 @@ Term timesField(const RHSExpr& lhs, const ScalarField& f, const ScalarField& lay
         materialiseCPU(lhs, s, S, pool);
         mul_host(rhs, s, pf->curr.data(), c, G);
     };
+    auto info = std::make_shared<fuse::Info>();
+    info->kind = fuse::Info::TIMES_FIELD;
+    info->inner = std::make_shared<RHSExpr>(lhs);
+    info->field = pf;
+    out.fusion = info;
     return out;
 }
 
@@ -241,6 +246,11 @@ Term timesExpr(const RHSExpr& a, const RHSExpr& b, const ScalarField& layout) {
         materialiseCPU(b, s2, S, pool);
         mul_host(rhs, s1, s2, c, G);
     };
+    auto info = std::make_shared<fuse::Info>();
+    info->kind = fuse::Info::TIMES_EXPR;
+    info->inner = std::make_shared<RHSExpr>(a);
+    info->inner2 = std::make_shared<RHSExpr>(b);
+    out.fusion = info;
     return out;
 }
 
@@ -320,6 +330,11 @@ Term grad(const ScalarField& f, int axis, double coeff) {
         check_rc(phix_grad_accumulate(d_rhs, pf->d_curr, c, axis, &grid, nullptr), "grad GPU kernel");
     };
     t.cpu_kernel = [pf, G, axis](double* rhs, double c, ScratchPool&) { grad_host(rhs, pf->curr.data(), c, axis, G); };
+    auto info = std::make_shared<fuse::Info>();
+    info->kind = fuse::Info::GRAD;
+    info->field = pf;
+    info->axis = axis;
+    t.fusion = info;
     return t;
 }
 

@@ -5,9 +5,13 @@
 // M*lap(such a sum, bcs) with the solver's own BCs, and every BC is a
 // PeriodicBC / NoFluxBC / FixedBC: each RK stage is then one fused kernel
 // (phix/detail/stage.cuh with the term program of the equation), the
-// multi-step Cahn-Hilliard form one kernel per step.  Anything else runs the
-// reference's sequence (Solver.cu:162-259, :317-340) on this library's
-// kernels: BC fills, one accumulate kernel per term, rk4 combination kernels.
+// multi-step Cahn-Hilliard form one kernel per step.  Other multi-step
+// systems, and Euler steps of other right-hand sides, compile each step into
+// a flat program (equation/FlatProgram.h: lap, grad, pw of up to three
+// fields, products) run as one kernel, with the BC fills in the reference's
+// order.  Anything else runs the reference's sequence (Solver.cu:162-259,
+// :317-340) on this library's kernels: BC fills, one accumulate kernel per
+// term, rk4 combination kernels.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -16,6 +20,7 @@
 #include <utility>
 
 #include "boundary/BoundaryCondition.h"
+#include "equation/FlatProgram.h"
 #include "equation/FusedStage.h"
 #include "phix_b200.h"
 #include "solver/Solver.h"
@@ -140,6 +145,16 @@ phix::Layout field_layout(const ScalarField& f) {
 }  // namespace
 
 // The compiled fused path.
+// One SolverStep of a general multi-step Solver compiled into one flat_step
+// launch (equation/FlatProgram.h), or left to the reference's sequence.
+struct FlatStepPlan {
+    bool fused = false;
+    fuse::FlatSpec spec;  // program and layout; field pointers are set at launch
+    const ScalarField* slots[fuse::FLAT_MAX_FIELDS] = {};
+    int nslots = 0;
+    std::shared_ptr<const fuse::FlatKernels> kern;
+};
+
 struct FusedPlan {
     std::shared_ptr<const fuse::PwKernels> kern;
     fuse::StageSpec spec;  // program, pattern, dim, layout; per-stage fields set at launch
@@ -147,11 +162,114 @@ struct FusedPlan {
     ScalarField* c = nullptr;   // multi-step: the TRANSIENT unknown
     ScalarField* mu = nullptr;  // multi-step: the STEADY unknown
     bool filled = false;        // the first step's full BC fill (padding ghosts) is done
+    std::vector<FlatStepPlan> flat;  // general multi-step: one entry per SolverStep
 };
 
 static std::shared_ptr<const fuse::PwKernels> identity_kernels() {
     static auto k = std::make_shared<detail::PwKernelsImpl<IdentityFn>>(IdentityFn{});
     return k;
+}
+
+// The flat program of a right-hand side (equation/FlatProgram.h): the terms
+// in order, products as nested sub-programs; false when a term is not one the
+// program holds, a second pw functor appears, or the fields differ in layout.
+class FlatBuilder {
+public:
+    FlatBuilder(FlatStepPlan& P, const ScalarField& layout) : P_(P), u_(layout) {}
+    bool expr(const RHSExpr& e, int sp) {
+        for (const auto& t : e.terms) {
+            if (!t.fusion) return false;
+            const fuse::Info& I = *t.fusion;
+            switch (I.kind) {
+                case fuse::Info::LAP:
+                case fuse::Info::GRAD: {
+                    const int k = slot(I.field);
+                    if (k < 0 || !push(I.kind == fuse::Info::LAP ? fuse::FL_LAP : fuse::FL_GRAD, k, I.axis, t.coeff))
+                        return false;
+                    break;
+                }
+                case fuse::Info::PW1:
+                case fuse::Info::PWN: {
+                    if (P_.kern || !I.flat || I.nargs < 1 || I.nargs > 3) return false;  // one functor per program
+                    P_.kern = I.flat;
+                    for (int a = 0; a < I.nargs; ++a)
+                        if ((P_.spec.pw_slot[a] = slot(I.args[a])) < 0) return false;
+                    if (!push(fuse::FL_PW, 0, 0, t.coeff)) return false;
+                    break;
+                }
+                case fuse::Info::TIMES_FIELD: {
+                    if (sp + 1 > fuse::FLAT_MAX_DEPTH || !push(fuse::FL_ZERO, 0, 0, 0.0) || !expr(*I.inner, sp + 1))
+                        return false;
+                    const int k = slot(I.field);
+                    if (k < 0 || !push(fuse::FL_MULF, k, 0, t.coeff)) return false;
+                    break;
+                }
+                case fuse::Info::TIMES_EXPR:
+                    if (sp + 2 > fuse::FLAT_MAX_DEPTH || !push(fuse::FL_ZERO, 0, 0, 0.0) || !expr(*I.inner, sp + 1) ||
+                        !push(fuse::FL_ZERO, 0, 0, 0.0) || !expr(*I.inner2, sp + 2) || !push(fuse::FL_MUL2, 0, 0, t.coeff))
+                        return false;
+                    break;
+                default:
+                    return false;
+            }
+        }
+        return true;
+    }
+    bool reads(const ScalarField* f) const {
+        for (int k = 0; k < P_.nslots; ++k)
+            if (P_.slots[k] == f) return true;
+        return false;
+    }
+
+private:
+    FlatStepPlan& P_;
+    const ScalarField& u_;
+    bool push(int kind, int field, int axis, double c) {
+        if (P_.spec.nops >= fuse::FLAT_MAX_OPS) return false;
+        P_.spec.op[P_.spec.nops++] = fuse::FlatOp{kind, field, axis, c};
+        return true;
+    }
+    int slot(const ScalarField* f) {
+        if (!f) return -1;
+        for (int k = 0; k < P_.nslots; ++k)
+            if (P_.slots[k] == f) return k;
+        if (P_.nslots >= fuse::FLAT_MAX_FIELDS || f->ghost != u_.ghost) return -1;
+        for (int a = 0; a < 3; ++a)
+            if (f->mesh.n[a] != u_.mesh.n[a] || f->mesh.d[a] != u_.mesh.d[a] || f->storedDims[a] != u_.storedDims[a])
+                return -1;
+        P_.slots[P_.nslots] = f;
+        return P_.nslots++;
+    }
+};
+
+static std::shared_ptr<const fuse::FlatKernels> identity_flat() {
+    static auto k = std::make_shared<fuse::FlatKernelsImpl<IdentityFn, 0>>(IdentityFn{});
+    return k;
+}
+
+// A SolverStep as one flat_step launch, where its right-hand side compiles.
+static void plan_flat_step(const SolverStep& s, FlatStepPlan& P) {
+    P = FlatStepPlan{};
+    const ScalarField& u = s.equation->unknown;
+    if (!s.equation->hasRHS() || u.mesh.dim < 1 || u.mesh.dim > 3) return;
+    FlatBuilder b(P, u);
+    P.spec.op[P.spec.nops++] = fuse::FlatOp{fuse::FL_ZERO, 0, 0, 0.0};
+    if (!b.expr(s.equation->rhsExpr(), 1)) return;
+    const bool transient = s.type == EquationType::TRANSIENT;
+    // a STEADY unknown is zeroed before its own right-hand side runs
+    if (!transient && b.reads(&u)) return;
+    if (transient && !u.d_prev) return;
+    fuse::FlatSpec& S = P.spec;
+    S.L = field_layout(u);
+    S.dim = u.mesh.dim;
+    for (int a = 0; a < 3; ++a) {
+        S.sdims[a] = u.storedDims[a];
+        S.i2[a] = a < S.dim ? 1.0 / (u.mesh.d[a] * u.mesh.d[a]) : 0.0;
+        S.inv2d[a] = a < S.dim ? 0.5 / u.mesh.d[a] : 0.0;
+    }
+    S.transient = transient ? 1 : 0;
+    if (!P.kern) P.kern = identity_flat();
+    P.fused = true;
 }
 
 // Single-equation plan, or null.
@@ -180,8 +298,23 @@ static std::unique_ptr<FusedPlan> plan_single(const Equation& eq, const std::vec
     return P;
 }
 
+// General multi-step plan: every step that compiles runs as one flat_step
+// launch; null when none does.
+static std::unique_ptr<FusedPlan> plan_multistep_flat(const std::vector<SolverStep>& steps, double dt) {
+    auto P = std::make_unique<FusedPlan>();
+    P->flat.resize(steps.size());
+    bool any = false;
+    for (std::size_t i = 0; i < steps.size(); ++i) {
+        plan_flat_step(steps[i], P->flat[i]);
+        P->flat[i].spec.dt = dt;
+        any = any || P->flat[i].fused;
+    }
+    if (!any) return nullptr;
+    return P;
+}
+
 // Multi-step Cahn-Hilliard plan: [mu STEADY <- program(c); c TRANSIENT <- M lap(mu)].
-static std::unique_ptr<FusedPlan> plan_multistep(const std::vector<SolverStep>& steps) {
+static std::unique_ptr<FusedPlan> plan_multistep_ch(const std::vector<SolverStep>& steps) {
     if (steps.size() != 2 || steps[0].type != EquationType::STEADY || steps[1].type != EquationType::TRANSIENT)
         return nullptr;
     ScalarField& mu = steps[0].equation->unknown;
@@ -232,6 +365,18 @@ Solver::Solver(Equation& equation, std::vector<BoundaryCondition*> bcs, double d
     if (!equation_.unknown.deviceAllocated())
         throw std::runtime_error("Solver: equation.unknown must have device memory allocated before constructing the Solver.");
     if (equation_.hasRHS()) plan_ = plan_single(equation_, bcs_);
+    if (!plan_ && !use_rk4_ && equation_.hasRHS()) {
+        // an Euler step whose terms the stage kernels do not take (grad, div,
+        // products, pw of several fields): the step {BCs on the unknown; rhs;
+        // u += dt rhs} as one flat_step launch where the terms compile
+        std::vector<SolverStep> one = {{&equation_.unknown, bcs_, &equation_, EquationType::TRANSIENT}};
+        auto P = plan_multistep_flat(one, dt);
+        if (P && P->flat[0].fused) {
+            steps_ = std::move(one);
+            stepScratch_.push_back(nullptr);
+            plan_ = std::move(P);
+        }
+    }
 }
 
 Solver::Solver(std::vector<SolverStep> steps, double dt_, TimeScheme scheme_)
@@ -259,7 +404,10 @@ Solver::Solver(std::vector<SolverStep> steps, double dt_, TimeScheme scheme_)
     }
     bool all_rhs = true;
     for (auto& s : steps_) all_rhs = all_rhs && s.equation->hasRHS();
-    if (all_rhs) plan_ = plan_multistep(steps_);
+    if (all_rhs) {
+        plan_ = plan_multistep_ch(steps_);
+        if (!plan_) plan_ = plan_multistep_flat(steps_, dt);
+    }
 }
 
 Solver::~Solver() = default;
@@ -396,6 +544,47 @@ void Solver::multiStepAdvanceCPU() {
 // and d_prev swap (d_prev keeps the previous time level).
 void Solver::fusedAdvance() {
     FusedPlan& P = *plan_;
+    if (!P.flat.empty()) {
+        // general multi-step: the reference's step order (Solver.cu:317-340),
+        // each compiled step one flat_step launch; a TRANSIENT step writes the
+        // unknown's other level and swaps it in (d_prev keeps the old level)
+        for (std::size_t i = 0; i < steps_.size(); ++i) {
+            auto& s = steps_[i];
+            for (auto* bc : s.bcs) bc->applyOnGPU(*s.sourceField);
+            FlatStepPlan& F = P.flat[i];
+            ScalarField& u = s.equation->unknown;
+            if (!F.fused) {
+                if (s.type == EquationType::STEADY) {
+                    s.equation->computeRHS(u);
+                } else {
+                    s.equation->computeRHS(*stepScratch_[i]);
+                    axpy(u.d_curr, stepScratch_[i]->d_curr, dt, u.storedSize);
+                    cuda_check(cudaDeviceSynchronize(), "Solver::multiStepAdvanceGPU");
+                }
+                continue;
+            }
+            fuse::FlatSpec S = F.spec;
+            for (int k = 0; k < F.nslots; ++k) {
+                S.f[k] = F.slots[k]->d_curr;
+                if (!S.f[k]) throw std::runtime_error("Solver: a field of step " + std::to_string(i) + " is not on device");
+            }
+            if (S.transient) {
+                S.u = u.d_curr;
+                S.out = u.d_prev;
+            } else {
+                S.out = u.d_curr;
+            }
+            if (F.kern->launch(S, nullptr) != PHIX_OK)
+                throw std::runtime_error(std::string("Solver: fused step launch failed: ") +
+                                         cudaGetErrorString(cudaGetLastError()));
+            phix::count_launch(1);
+            if (S.transient) std::swap(u.d_curr, u.d_prev);
+        }
+        for (std::size_t i = 0; i < steps_.size(); ++i)
+            if (steps_[i].type == EquationType::TRANSIENT && !P.flat[i].fused)
+                steps_[i].equation->unknown.advanceTimeLevelGPU();
+        return;
+    }
     fuse::StageSpec S = P.spec;
     phix::StageArgs<double>& A = S.A;
     ScalarField& u = P.multistep ? *P.c : equation_.unknown;

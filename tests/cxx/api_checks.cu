@@ -8,6 +8,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <fstream>
 #include <functional>
 #include <iterator>
@@ -205,6 +206,148 @@ int main() {
         char buf[128];
         std::snprintf(buf, sizeof buf, "mass of c %.15e -> %.15e (rel %.2e)", m0, m1, std::fabs(m1 - m0) / m0);
         report("VectorSolver coupled RK4, conserved c", finite && std::fabs(m1 - m0) / m0 < 1e-12, buf);
+    }
+    // 9. General multi-step Solver (the glass-formation application's form):
+    //    mu and D STEADY from pw terms of 2 and 3 fields, c TRANSIENT from
+    //    D lap(mu) + grad(D) . grad(mu), phi and eta TRANSIENT from a pw term
+    //    plus lap; every step one fused launch.  All stored cells of the five
+    //    fields, fused against the unfused sequence, bit for bit.
+    for (int dim = 2; dim <= 3; ++dim) {
+        Mesh mesh = dim == 2 ? Mesh::makeUniform2D(CoordSys::CARTESIAN, 96, 1.0, 0.0, 70, 0.8, 0.0)
+                             : Mesh::makeUniform3D(CoordSys::CARTESIAN, 40, 1.0, 0.0, 24, 1.0, 0.0, 18, 1.2, 0.0);
+        auto f2 = [] __host__ __device__(double cv, double pv) { return (1.0 - pv * pv) * (cv - 0.5) * 2.5; };
+        auto f3 = [] __host__ __device__(double cv, double pv, double ev) {
+            return (0.3 + 0.5 * pv + 0.2 * ev * ev) * cv * (1.0 - cv);
+        };
+        auto g3 = [] __host__ __device__(double pv, double ev, double cv) {
+            return -0.8 * (pv * (1.0 - pv) * (0.5 - pv + 0.1 * cv) + 0.3 * pv * ev * ev);
+        };
+        auto h2 = [] __host__ __device__(double pv, double ev) { return -0.6 * (ev * (1.0 - ev) * (0.5 - ev) + 0.2 * pv * pv * ev); };
+        std::vector<double> got[2][5];
+        bool fused_ok = true;
+        for (int fused = 1; fused >= 0; --fused) {
+            ScalarField c(mesh, "c"), phi(mesh, "phi"), eta(mesh, "eta"), mu(mesh, "mu"), D(mesh, "D");
+            fill_random(c, 0.3, 0.7, 41);
+            fill_random(phi, 0.0, 1.0, 42);
+            fill_random(eta, 0.0, 0.4, 43);
+            ScalarField* all[5] = {&c, &phi, &eta, &mu, &D};
+            for (auto* f : all) {
+                f->allocDevice();
+                f->uploadAllToDevice();
+            }
+            PeriodicBC bx(Axis::X), bz(Axis::Z);
+            NoFluxBC by(Axis::Y);
+            std::vector<BoundaryCondition*> bcs = {&bx, &by};
+            if (dim == 3) bcs.push_back(&bz);
+            Equation eq_mu(mu, "mu"), eqD(D, "D"), eqC(c, "c"), eqPhi(phi, "phi"), eqEta(eta, "eta");
+            eq_mu.setRHS(pw(c, phi, f2));
+            eqD.setRHS(pw(c, phi, eta, f3));
+            RHSExpr rc = RHSExpr(D * lap(mu)) + grad(D, 0) * grad(mu, 0) + grad(D, 1) * grad(mu, 1);
+            if (dim == 3) rc += grad(D, 2) * grad(mu, 2);
+            eqC.setRHS(rc);
+            eqPhi.setRHS(pw(phi, eta, c, g3) + 0.3 * lap(phi));
+            eqEta.setRHS(pw(phi, eta, h2) + 0.2 * lap(eta));
+            Solver s({{&c, bcs, &eq_mu, EquationType::STEADY},
+                      {&mu, bcs, &eqD, EquationType::STEADY},
+                      {&D, bcs, &eqD, EquationType::STEADY},
+                      {&c, bcs, &eqC, EquationType::TRANSIENT},
+                      {&phi, bcs, &eqPhi, EquationType::TRANSIENT},
+                      {&eta, bcs, &eqEta, EquationType::TRANSIENT}},
+                     2e-3, TimeScheme::EULER);
+            if (fused) fused_ok = s.fused();
+            else s.disableFusion();
+            s.run(20);
+            for (int q = 0; q < 5; ++q) {
+                all[q]->downloadCurrFromDevice();
+                got[fused][q] = all[q]->curr;
+            }
+        }
+        bool same = fused_ok;
+        const char* names[5] = {"c", "phi", "eta", "mu", "D"};
+        std::string which;
+        for (int q = 0; q < 5; ++q) {
+            bool eq = got[0][q].size() == got[1][q].size();
+            for (std::size_t i = 0; eq && i < got[0][q].size(); ++i)
+                eq = std::memcmp(&got[0][q][i], &got[1][q][i], sizeof(double)) == 0;
+            if (!eq) which += std::string(" ") + names[q];
+            same = same && eq;
+        }
+        report(std::string("general multi-step, 6 steps, 5 fields, ") + (dim == 2 ? "2-D" : "3-D"), same,
+               fused_ok ? (which.empty() ? "every stored cell equal, fused vs unfused" : "differs:" + which)
+                        : "the solver did not fuse");
+    }
+    // 11. Single-equation Euler with gradient, product and two-field pw terms
+    //     (one flat_step launch per step), zero-flux x, periodic y
+    {
+        Mesh mesh = Mesh::makeUniform2D(CoordSys::CARTESIAN, 77, 1.0, 0.0, 45, 0.9, 0.0);
+        ScalarField v(mesh, "v");
+        fill_random(v, 0.2, 0.8, 61);
+        v.allocDevice();
+        v.uploadAllToDevice();
+        fused_vs_unfused("Euler, lap + grad*grad + pw(u, v) + grad(v) + u*lap(v)", mesh, 0.2, 0.8, 40,
+                         [&](ScalarField& u, bool fused, int n) {
+                             NoFluxBC bx(Axis::X);
+                             PeriodicBC by(Axis::Y);
+                             Equation eq(u, "u");
+                             eq.setRHS(RHSExpr(0.5 * lap(u)) + 0.2 * (grad(u, 0) * grad(u, 1)) +
+                                       pw(u, v, [] __host__ __device__(double a, double b) { return a * (1.0 - a) * (b - 0.5); }) +
+                                       grad(v, 0, 0.1) + u * lap(v));
+                             Solver s(eq, {&bx, &by}, 0.01, TimeScheme::EULER);
+                             if (!fused) s.disableFusion();
+                             if (fused && !s.fused()) report("Euler flat plan", false, "the solver did not fuse");
+                             s.run(n);
+                         });
+    }
+    // 10. The same six-step system at 1024^2: ms per time step, fused against
+    //     the unfused sequence (one kernel per term, scratch materialisation,
+    //     as the reference launches it)
+    {
+        Mesh mesh = Mesh::makeUniform2D(CoordSys::CARTESIAN, 1024, 1.0, 0.0, 1024, 1.0, 0.0);
+        auto f2 = [] __host__ __device__(double cv, double pv) { return (1.0 - pv * pv) * (cv - 0.5) * 2.5; };
+        auto f3 = [] __host__ __device__(double cv, double pv, double ev) {
+            return (0.3 + 0.5 * pv + 0.2 * ev * ev) * cv * (1.0 - cv);
+        };
+        auto g3 = [] __host__ __device__(double pv, double ev, double cv) {
+            return -0.8 * (pv * (1.0 - pv) * (0.5 - pv + 0.1 * cv) + 0.3 * pv * ev * ev);
+        };
+        auto h2 = [] __host__ __device__(double pv, double ev) { return -0.6 * (ev * (1.0 - ev) * (0.5 - ev) + 0.2 * pv * pv * ev); };
+        double ms[2] = {0.0, 0.0};
+        for (int fused = 0; fused < 2; ++fused) {
+            ScalarField c(mesh, "c"), phi(mesh, "phi"), eta(mesh, "eta"), mu(mesh, "mu"), D(mesh, "D");
+            fill_random(c, 0.3, 0.7, 51);
+            fill_random(phi, 0.0, 1.0, 52);
+            fill_random(eta, 0.0, 0.4, 53);
+            for (ScalarField* f : {&c, &phi, &eta, &mu, &D}) {
+                f->allocDevice();
+                f->uploadAllToDevice();
+            }
+            PeriodicBC bx(Axis::X);
+            NoFluxBC by(Axis::Y);
+            std::vector<BoundaryCondition*> bcs = {&bx, &by};
+            Equation eq_mu(mu, "mu"), eqD(D, "D"), eqC(c, "c"), eqPhi(phi, "phi"), eqEta(eta, "eta");
+            eq_mu.setRHS(pw(c, phi, f2));
+            eqD.setRHS(pw(c, phi, eta, f3));
+            eqC.setRHS(RHSExpr(D * lap(mu)) + grad(D, 0) * grad(mu, 0) + grad(D, 1) * grad(mu, 1));
+            eqPhi.setRHS(pw(phi, eta, c, g3) + 0.3 * lap(phi));
+            eqEta.setRHS(pw(phi, eta, h2) + 0.2 * lap(eta));
+            Solver s({{&c, bcs, &eq_mu, EquationType::STEADY},
+                      {&mu, bcs, &eqD, EquationType::STEADY},
+                      {&D, bcs, &eqD, EquationType::STEADY},
+                      {&c, bcs, &eqC, EquationType::TRANSIENT},
+                      {&phi, bcs, &eqPhi, EquationType::TRANSIENT},
+                      {&eta, bcs, &eqEta, EquationType::TRANSIENT}},
+                     1e-4, TimeScheme::EULER);
+            if (!fused) s.disableFusion();
+            s.run(5);
+            const int n = 100;
+            const auto t0 = std::chrono::steady_clock::now();
+            s.run(n);
+            ms[fused] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / n;
+        }
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "1024^2, 6 steps over 5 fields: unfused %.3f ms, fused %.3f ms per time step (%.1fx)",
+                      ms[0], ms[1], ms[0] / ms[1]);
+        report("general multi-step timing", ms[1] > 0.0, buf);
     }
     // 7. OutputWriter: the asynchronous files equal IO::writeField's byte for
     //    byte, for a snapshot taken before the device cells change again

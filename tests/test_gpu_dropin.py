@@ -13,6 +13,11 @@ write the same fields bit for bit.
     asynchronous OutputWriter and with "async": false (the reference's
     synchronous order); those two runs must write the same bytes, and both
     must match the reference's files to 1e-12.
+  * applications/solvers/glass_formation/2D/GFA.cu: the glass-formation
+    application (six SolverSteps over c, phi, eta, mu, D: pw terms of two
+    and three fields, D lap(mu) + grad(D) . grad(mu), pw + lap), which runs
+    as one fused launch per step here; its files must equal the reference's
+    byte for byte.
 
 The binaries are built where the reference tree exists; without them the
 tests skip.
@@ -153,3 +158,55 @@ def test_ch_app_output_identical(cuda, tmp_path):
             assert _numbers_close(a, b, 1e-12), f"{n}: text differs beyond 1e-12"
     assert worst <= 1e-12, worst
     print(f"CH app: {len(names)} files, async == sync byte for byte, max-abs vs reference {worst:.1e}")
+
+
+GFA_SETTINGS = """{{
+    // written by tests/test_gpu_dropin.py; constants of an Fe-B alloy
+    "mesh": {{"nx": {nx}, "ny": {ny}, "dx": 3.0e-4, "dy": 3.0e-4, "x0": 0.0, "y0": 0.0}},
+    "initialize": {{"start_from": "initial_field", "dt": 1.0e-6, "nSteps": {nsteps}}},
+    "boundary_conditions": {{"x_min": "NoFlux", "x_max": "NoFlux", "y_min": "NoFlux", "y_max": "NoFlux"}},
+    "constants": {{"M_eta": 1.0, "D_Am": 3.0e-12, "eps_sq": 2.86e-3, "beta_sq": 1.0e-4, "w_phi": 441.0,
+                   "w_eta": 10.0, "w_ex": 100.0, "T": 1000.0, "T_g": 710.0, "alpha": 0.45,
+                   "V_m_L": 2.64e-5, "V_m_S": 2.44e-5}},
+    "output": {{"print_interval": {every}, "write_interval": {every}, "format": "ALL"}}
+}}
+"""
+
+
+def test_gfa_app_identical(cuda, tmp_path):
+    exes = {"ref": _bin("gfa_ref"), "ours": _bin("gfa_phix")}
+    nx, ny, nsteps, every = 96, 64, 300, 100
+    # an amorphous matrix (eta = 1, c = 0.25) around a crystalline disc of
+    # radius 3 cells (phi = 1, eta = 0, c = 0.33 + noise)
+    rng = np.random.default_rng(5)
+    jj, ii = np.mgrid[0:ny, 0:nx]
+    disc = (ii + 0.5 - nx / 2) ** 2 + (jj + 0.5 - ny / 2) ** 2 <= 9.0
+    c0 = np.where(disc, 0.33 + rng.uniform(-0.01, 0.01, size=(ny, nx)), 0.25)
+    phi0 = np.where(disc, 1.0, 0.0)
+    eta0 = np.where(disc, 0.0, 1.0)
+    out, files, logs = {}, {}, {}
+    for tag, exe in exes.items():
+        d = tmp_path / tag
+        (d / "settings" / "initial_field").mkdir(parents=True)
+        (d / "settings" / "settings.jsonc").write_text(GFA_SETTINGS.format(nx=nx, ny=ny, nsteps=nsteps, every=every))
+        for name, a in (("c", c0), ("phi", phi0), ("eta", eta0), ("mu", np.zeros_like(c0))):
+            _write_field(d / "settings" / "initial_field" / f"{name}.field", name, a)
+        rc, text = _run(exe, d)
+        assert rc == 0, text[-2000:]
+        logs[tag] = text.splitlines()
+        out[tag] = [l for l in text.splitlines() if "written:" in l]
+        files[tag] = {n: (d / "output" / n).read_bytes() for n in sorted(os.listdir(d / "output"))}
+    names = sorted(files["ref"])
+    assert sorted(files["ours"]) == names and len(names) == 3 * 3 * (nsteps // every + 1)
+    assert out["ours"] == out["ref"]
+    worst = 0.0
+    for n in names:
+        a, b = files["ref"][n], files["ours"][n]
+        if n.endswith(".field"):
+            cut = a.index(b"---\n") + 4
+            da, db = np.frombuffer(a[cut:], "<f8"), np.frombuffer(b[cut:], "<f8")
+            assert np.isfinite(da).all(), f"{n}: the reference wrote non-finite values\n" + "\n".join(logs["ref"][-12:])
+            worst = max(worst, float(np.abs(da - db).max()))
+    for n in names:
+        assert files["ours"][n] == files["ref"][n], f"{n}: differs from the reference (field max-abs {worst:.3e})"
+    print(f"GFA app: {len(names)} files identical to the reference's")
