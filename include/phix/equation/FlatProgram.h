@@ -63,15 +63,23 @@ struct FlatKernels {
     virtual int launch(const FlatSpec& spec, void* stream) const = 0;
 };
 
-// F is called with NA arguments (NA = 0: the program has no pw term).
+// F is called with NA arguments (NA = 0: the program has no pw term).  The
+// value stack (at most FLAT_MAX_DEPTH = 4 deep, which the program builder
+// enforces) lives in four registers: t is the top, s1..s3 the values below;
+// a push or pop shifts them, so no stack slot is indexed at run time.
 template <class F, int NA>
 __device__ __forceinline__ double flat_eval(const FlatSpec& S, const F& func, int c) {
-    double st[FLAT_MAX_DEPTH];
-    int sp = 0;
+    static_assert(FLAT_MAX_DEPTH == 4, "the register stack holds four values");
+    double t = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
     for (int q = 0; q < S.nops; ++q) {
         const FlatOp o = S.op[q];
         switch (o.kind) {
-            case FL_ZERO: st[sp++] = 0.0; break;
+            case FL_ZERO:
+                s3 = s2;
+                s2 = s1;
+                s1 = t;
+                t = 0.0;
+                break;
             case FL_LAP: {
                 const double* f = S.f[o.field];
                 const double f2 = phix::rmul(2.0, f[c]);
@@ -88,13 +96,13 @@ __device__ __forceinline__ double flat_eval(const FlatSpec& S, const F& func, in
                         v = phix::lap_combine<double, 3>(tx, ty, tz, S.i2[0], S.i2[1], S.i2[2]);
                     }
                 }
-                st[sp - 1] = phix::rfma(o.c, v, st[sp - 1]);
+                t = phix::rfma(o.c, v, t);
                 break;
             }
             case FL_GRAD: {
                 const double* f = S.f[o.field];
                 const int off = S.L.s[o.axis];
-                st[sp - 1] = phix::rfma(phix::rmul(o.c, phix::rsub(f[c + off], f[c - off])), S.inv2d[o.axis], st[sp - 1]);
+                t = phix::rfma(phix::rmul(o.c, phix::rsub(f[c + off], f[c - off])), S.inv2d[o.axis], t);
                 break;
             }
             case FL_PW: {
@@ -102,23 +110,28 @@ __device__ __forceinline__ double flat_eval(const FlatSpec& S, const F& func, in
                 if constexpr (NA == 1) v = func(S.f[S.pw_slot[0]][c]);
                 else if constexpr (NA == 2) v = func(S.f[S.pw_slot[0]][c], S.f[S.pw_slot[1]][c]);
                 else if constexpr (NA == 3) v = func(S.f[S.pw_slot[0]][c], S.f[S.pw_slot[1]][c], S.f[S.pw_slot[2]][c]);
-                st[sp - 1] = __fma_rn(o.c, v, st[sp - 1]);
+                t = __fma_rn(o.c, v, t);
                 break;
             }
-            case FL_MULF: {
-                const double s = st[--sp];
-                st[sp - 1] = phix::rfma(phix::rmul(o.c, s), S.f[o.field][c], st[sp - 1]);
+            case FL_MULF: {  // pop the materialised operand, fold into the value below
+                const double m = t;
+                t = s1;
+                s1 = s2;
+                s2 = s3;
+                t = phix::rfma(phix::rmul(o.c, m), S.f[o.field][c], t);
                 break;
             }
-            default: {  // FL_MUL2
-                const double s2 = st[--sp];
-                const double s1 = st[--sp];
-                st[sp - 1] = phix::rfma(phix::rmul(o.c, s1), s2, st[sp - 1]);
+            default: {  // FL_MUL2: pop two materialised operands
+                const double m2 = t, m1 = s1;
+                t = s2;
+                s1 = s3;
+                s2 = 0.0;
+                t = phix::rfma(phix::rmul(o.c, m1), m2, t);
                 break;
             }
         }
     }
-    return st[0];
+    return t;
 }
 
 // One thread per stored cell: x along the stored row, y over the stored rows
