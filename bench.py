@@ -147,6 +147,7 @@ TRAFFIC = {
     ("ch2d", "f64", "stage_box"): 12.63e6,  # profiles/stage_box_ch1024_f64.md: mean of stage 1 and 2 launches
     ("ch2d", "f32", "step_box"): 8.47e6,    # profiles/step_box_ch1024_f32.md
     ("batch", "f32", "step_pair_batched"): 358.3e6,  # profiles/step_pair_batched_batch64_f32.md
+    ("ch2d_ms", "f64", "step_pair_ms"): 8.45e6,  # profiles/step_pair_ms_ch1024_f64.md
 }
 
 # step tiles 6 and up are the pair kernels (include/phix_b200.h, phix_stepper_set_tiles)
