@@ -39,7 +39,9 @@ struct PolUser {
     // rhs = 0; rhs += c_i * op_i  (Equation::computeRHS order)
     __device__ __forceinline__ double program(double y, double lapy) const {
         double acc = 0.0;
-        for (int i = 0; i < nops; ++i) {
+#pragma unroll
+        for (int i = 0; i < MAX_OPS; ++i) {  // unrolled: no run-time trip count
+            if (i >= nops) break;
             const double v = op[i] == OP_LAP ? lapy : (double)f(y);
             acc = __fma_rn(c[i], v, acc);
         }
