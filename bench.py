@@ -9,15 +9,15 @@ c0 = 0.5 + U[-0.01, 0.01] (seed 1).
 
 One bench "step" = one output interval: STEPS_PER_INTERVAL RK4 time steps of
 the whole field, replayed from a CUDA graph (the library's default launch
-shape: one launch per stage in FP64, one per time step in FP32; --launch
-overrides it).  --workload selects the other configurations (ac2d, chac3d,
+shape: one launch per RK4 time step in FP64 and FP32; --launch overrides it).  --workload selects the other configurations (ac2d, chac3d,
 batch, and ch2d_ms: the CH application's multi-step form), reported with
 the same keys.  L2 is flushed (256 MiB write) between timed steps, outside the timed
 events.  `value` = cell-updates/s = cells x time steps / device time.
 `e2e` runs the same interval through the C ABI with pinned HOST buffers
 (phix_stepper_run_host: H2D, advance, D2H, synchronise) inside the timed
 region.  Multi-GPU: independent replicas, one per rank (the single-field
-configs do not shard; scaling "weak"), time = max over ranks.
+configs do not shard; scaling "weak"), time = max over ranks.  `--gpus N`
+without a launcher starts N ranks itself (torchrun on 127.0.0.1).
 """
 from __future__ import annotations
 
@@ -121,6 +121,43 @@ def reference_cpu_rate(fields, g, phys, prm, scheme, dt, nsteps):
     return cells * nsteps / el, el
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def openmp_cpu_rate(fields, g, phys, prm, scheme, dt, min_seconds=3.0, max_steps=1000):
+    """The oracle's restatement of the same discretisation built with OpenMP
+    (oracle/liboracle_omp.so) on all host threads, in the device build's
+    rounding pattern (fma_mode 1): time steps are run in growing chunks until
+    `min_seconds` of wall time.  Returns (cell-updates/s, seconds, steps,
+    threads)."""
+    from oracle.oracle import LIB_ORACLE_OMP, Grid, Oracle
+    from phix_b200 import MULTISTEP
+    omp = Oracle(LIB_ORACLE_OMP)
+    grid = Grid(n=tuple(g.n[a] for a in range(g.dim)), d=tuple(g.d[a] for a in range(g.dim)), ghost=g.ghost,
+                bc=tuple(g.bc_type), bc_val=tuple(g.bc_val), fma_mode=1)
+    work = [f.copy() for f in fields]
+    cells = g.n[0] * g.n[1] * g.n[2] * (1 if scheme == MULTISTEP else len(fields))
+    done, el, chunk = 0, 0.0, 1
+    while el < min_seconds and done < max_steps:
+        t0 = time.perf_counter()
+        if scheme == MULTISTEP:
+            omp.advance_ch_multistep(work[0], work[1], prm, dt, chunk, grid)
+        else:
+            omp.advance(work, phys, prm, scheme, dt, chunk, grid)
+        el += time.perf_counter() - t0
+        done += chunk
+        chunk = min(2 * chunk, max_steps - done) or 1
+    return cells * done / el, el, done, omp.threads()
+
+
 # ---------------------------------------------------------------------------
 # workloads: each runner advances its whole field(s) by `K` time steps per
 # bench step and knows its algorithmic bytes and its end-to-end path
@@ -138,16 +175,16 @@ WORKLOADS = {
               "synthetic: per-instance size/kappa/M/mean from numpy default_rng(3)"),
 }
 
-# DRAM bytes (read + write) per launch of the dominant kernel, from the ncu
-# captures summarised under profiles/ (cold L2, so an upper bound for the
-# graph-replayed launches); keyed by (workload, dtype, launches per time step).
+# DRAM bytes (read + write) per launch of the dominant kernel, from one ncu
+# capture of each (cold L2, so an upper bound for the graph-replayed
+# launches); keyed by (workload, dtype, kernel).
 TRAFFIC = {
-    ("ch2d", "f64", "step_pair"): 8.46e6,   # profiles/step_pair_ch1024_f64.md
-    ("ch2d", "f32", "step_pair"): 8.46e6,   # profiles/step_pair_ch1024_f32.md
-    ("ch2d", "f64", "stage_box"): 12.63e6,  # profiles/stage_box_ch1024_f64.md: mean of stage 1 and 2 launches
-    ("ch2d", "f32", "step_box"): 8.47e6,    # profiles/step_box_ch1024_f32.md
-    ("batch", "f32", "step_pair_batched"): 358.3e6,  # profiles/step_pair_batched_batch64_f32.md
-    ("ch2d_ms", "f64", "step_pair_ms"): 8.45e6,  # profiles/step_pair_ms_ch1024_f64.md
+    ("ch2d", "f64", "step_pair"): 8.46e6,   # CH 1024^2 RK4, one launch per step
+    ("ch2d", "f32", "step_pair"): 8.46e6,
+    ("ch2d", "f64", "stage_box"): 12.63e6,  # mean of the stage-1 and stage-2 launches
+    ("ch2d", "f32", "step_box"): 8.47e6,
+    ("batch", "f32", "step_pair_batched"): 358.3e6,  # 64 instances, one launch per step
+    ("ch2d_ms", "f64", "step_pair_ms"): 8.45e6,  # CH 1024^2 multi-step Euler
 }
 
 # step tiles 6 and up are the pair kernels (include/phix_b200.h, phix_stepper_set_tiles)
@@ -217,6 +254,9 @@ class StepperRun:
     def cpu_sample(self, nsteps):
         return reference_cpu_rate(self.fields, self.g, self.phys, self.prm, self.scheme, self.dt, nsteps)
 
+    def cpu_sample_openmp(self):
+        return openmp_cpu_rate(self.fields, self.g, self.phys, self.prm, self.scheme, self.dt)
+
     def close(self):
         self.st.close()
 
@@ -283,8 +323,59 @@ class BatchRun:
         return reference_cpu_rate([self.fields[i]], self.grids[i], self.phys, self.prms[i], self.scheme, self.dt,
                                   nsteps)
 
+    def cpu_sample_openmp(self):
+        i = next(k for k, g in enumerate(self.grids) if g.n[0] == 256)
+        return openmp_cpu_rate([self.fields[i]], self.grids[i], self.phys, self.prms[i], self.scheme, self.dt)
+
     def close(self):
         self.b.close()
+
+
+def resolve_world(gpus: int, env=None) -> int:
+    """World size of this run: WORLD_SIZE when a launcher set it (it must
+    equal --gpus), else 1 (a single process; main() starts N ranks itself
+    for --gpus N > 1)."""
+    env = os.environ if env is None else env
+    if "WORLD_SIZE" not in env:
+        return 1
+    world = int(env["WORLD_SIZE"])
+    if world != gpus:
+        raise SystemExit(f"bench.py: --gpus {gpus} but the launcher started WORLD_SIZE={world} ranks")
+    return world
+
+
+def launcher_command(argv, gpus: int, port: int):
+    """The torchrun command that starts `gpus` ranks of this script on one
+    node with the same arguments (rendezvous on 127.0.0.1)."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+            "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+
+
+def free_port() -> int:
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def combine_over_ranks(total_ms: float, cells: float, e2e_ms: float, device, world: int):
+    """Job totals over the ranks: the slowest rank's timed-region and e2e
+    times (max) and the cells all ranks advanced (sum)."""
+    if world == 1:
+        return total_ms, cells, e2e_ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(cells)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t[0].item()), float(c[0].item()), float(t[1].item())
+
+
+def job_summary(world: int, steps: int, K: int, total_ms: float, job_cells: float) -> dict:
+    """The whole-job keys of the JSON line: `value` = cell-updates of all
+    ranks per second of the slowest rank's timed region."""
+    return {"n_gpus": world, "ms_per_step": total_ms / steps, "value": job_cells * K * steps / (total_ms / 1e3)}
 
 
 def bench_ours(args):
@@ -293,7 +384,7 @@ def bench_ours(args):
 
     import phix_b200 as px
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    world = resolve_world(args.gpus)
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
@@ -333,18 +424,9 @@ def bench_ours(args):
     if world > 1:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
-    job_cells = run.cells
-    if world > 1:
-        t = torch.tensor([float(run.cells)], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        job_cells = float(t.item())
-    value = job_cells * K * args.steps / (total_ms / 1e3)
+    total_ms, job_cells, _ = combine_over_ranks(sum(step_ms), run.cells, 0.0, dev, world)
+    job = job_summary(world, args.steps, K, total_ms, job_cells)
+    ms_per_step, value = job["ms_per_step"], job["value"]
 
     # roofline: algorithmic bytes of one time step (13w per field-cell for RK4,
     # the traffic of one launch per stage; 2w for Euler) over the device time
@@ -386,37 +468,44 @@ def bench_ours(args):
     torch.cuda.synchronize(dev)
     e2e_wall = time.perf_counter() - t0
     e2e_ms = max(e2e_dev.elapsed_time(e2e_dev2), 1e3 * e2e_wall)
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    _, _, e2e_ms = combine_over_ranks(0.0, 0.0, e2e_ms, dev, world)
     e2e_value = job_cells * K * e2e_steps / (e2e_ms / 1e3)
 
     line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
+            inst = " (one 256^2 instance)" if args.workload == "batch" else ""
+            try:
+                rate, el, n_omp, threads = run.cpu_sample_openmp()
+                cpu = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                       "cpu_model": cpu_model(), "nproc": os.cpu_count(),
+                       "sample": f"the oracle's C restatement of the same discretisation, OpenMP on {threads} "
+                                 f"host threads (oracle/liboracle_omp.so, device rounding pattern), {n_omp} time "
+                                 f"steps of the same workload{inst}, {el:.1f} s"}
+            except Exception as e:
+                cpu = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "port",
+                       "sample": f"unavailable: {e}"}
             try:
                 n_cpu = args.cpu_baseline_steps if args.workload != "chac3d" else 1
                 rate, el = run.cpu_sample(n_cpu)
                 if args.workload == "chac3d":
                     rate *= run.nf  # field-cell updates, like `value`
-                cpu = {"value": rate, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                       "sample": f"reference CPU path (computeRHSCPU + applyOnCPU, GPU stage semantics), "
-                                 f"{n_cpu} time steps of the same workload"
-                                 f"{' (one 256^2 instance)' if args.workload == 'batch' else ''}, "
-                                 f"{el:.1f} s, 1 thread"}
+                cpu["reference_1thread"] = {
+                    "value": rate, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                    "sample": f"reference CPU path (computeRHSCPU + applyOnCPU, GPU stage semantics), "
+                              f"{n_cpu} time steps of the same workload{inst}, {el:.1f} s, 1 thread (the "
+                              f"reference has no threading)"}
             except Exception as e:  # oracle/_ref not built on this machine
-                cpu = {"value": None, "unit": "cell-updates/s", "cores": 0, "kind": "reference",
-                       "sample": f"unavailable: {e}"}
+                cpu["reference_1thread"] = {"value": None, "sample": f"unavailable: {e}"}
         line = {
             "metric": METRIC,
-            "value": value,
+            "value": job["value"],
             "unit": "cell-updates/s",
-            "n_gpus": world,
+            "n_gpus": job["n_gpus"],
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": ms_per_step,
+            "ms_per_step": job["ms_per_step"],
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
@@ -628,6 +717,10 @@ def main():
     ap.add_argument("--autotune", action="store_true",
                     help="time every launch form and tile shape on the grid first (phix_stepper_autotune)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # --gpus N without a launcher: start N ranks of this script on this node
+        import subprocess as sp
+        raise SystemExit(sp.call(launcher_command(sys.argv[1:], args.gpus, free_port())))
     if args.impl == "ours":
         args.warmup = max(args.warmup, 3)  # timing rule: at least 3 untimed warm-up steps
     if args.impl == "reference":

@@ -36,6 +36,7 @@ extern "C" {
 #define PHIX_ERR_CUDA (-2)        /* CUDA runtime failure (std::runtime_error)     */
 #define PHIX_ERR_UNSUPPORTED (-3) /* combination not built                        */
 #define PHIX_ERR_NONFINITE (-4)   /* diagnostics found NaN/Inf in a field         */
+#define PHIX_ERR_TIMEOUT (-5)     /* a bounded device-side wait gave up           */
 
 /* boundary condition kinds, per axis side (Boundary.cu:95-195) */
 #define PHIX_BC_NONE 0     /* ghost cells left as stored                    */
@@ -290,6 +291,18 @@ int phix_surrogate_grad(phix_surrogate_t* s, const double* c, const double* c_ne
 int phix_surrogate_adam(phix_surrogate_t* s, const float* grads, float lr, void* stream);
 /* Device pointer of the internal FP32 gradient vector. */
 float* phix_surrogate_grad_ptr(phix_surrogate_t* s);
+/* Reads and clears the device error flag of the surrogate's tensor-core
+ * kernels: PHIX_ERR_TIMEOUT if one of their bounded mbarrier waits (2 s) gave
+ * up since the last check (the kernel then returned without its result),
+ * else PHIX_OK.  phix_surrogate_step is asynchronous and does not read the
+ * flag; phix_surrogate_grad reads it.  Synchronous on `stream`. */
+int phix_surrogate_status(phix_surrogate_t* s, void* stream);
+/* Self-test of those bounded waits: one thread waits for an mbarrier of count
+ * 1 with a wall-clock limit of limit_s (0 < limit_s <= 2), arriving on it
+ * first when `arrive` is non-zero.  Returns PHIX_OK when the wait completed and
+ * PHIX_ERR_TIMEOUT when it gave up (no arrival), the kernel having returned
+ * and the context still usable.  No reference counterpart. */
+int phix_wait_selftest(int arrive, double limit_s, void* stream);
 /* Copy the physical plane of a 2-D FP64 stored field to / from a compact
  * [H][W] array. */
 int phix_plane_gather(const double* stored, double* plane, int H, int W, int ghost, void* stream);
@@ -309,18 +322,21 @@ int phix_reduce_mass_energy(const double* const* fields, int phys, const double*
 int phix_stepper_diagnostics(phix_stepper_t* h, double* out);
 
 /* Allocation-free variant of phix_reduce_mass_energy, for callers that cannot
- * allocate device memory (code running while a CUDA graph is being captured,
- * hosts whose device memory is owned by another runtime or allocator,
- * real-time loops that forbid allocation).  It calls no cudaMalloc, cudaFree
- * or allocating library routine: its scratch is one triple per physical row
- * (n[1]*n[2] rows) in a file-scope device array sized for
- * PHIX_NOALLOC_MAX_ROWS rows (about 1.5 MiB, held on every GPU that loads the
- * library until exit); larger grids return PHIX_ERR_ARG.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress), so make
- * it before any stream capture.  All calls share the one array: calls that
- * overlap on the GPU race and must be serialised.  Synchronous; same outputs
- * and status codes as phix_reduce_mass_energy.  No counterpart in the
- * reference (which has no runtime diagnostics). */
+ * allocate device memory (hosts whose device memory is owned by another
+ * runtime or allocator, real-time loops that forbid allocation after
+ * start-up).  It calls no cudaMalloc, cudaFree or allocating library routine:
+ * its scratch is one triple per physical row (n[1]*n[2] rows) in a
+ * file-scope device array sized for PHIX_NOALLOC_MAX_ROWS rows (about
+ * 1.5 MiB, held on every GPU that loads the library until exit); larger grids
+ * return PHIX_ERR_ARG.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress) and keeps it for the life of the
+ * device's context (do not call it on a device after cudaDeviceReset there).
+ * All calls share the one array: calls that overlap on the GPU race and must
+ * be serialised.  Synchronous (a device-to-host copy and a wait on `stream`),
+ * so not for a stream under capture, nor for stream = NULL while a
+ * global-mode capture is active; same outputs and status codes as
+ * phix_reduce_mass_energy.  No counterpart in the reference (which has no
+ * runtime diagnostics). */
 #define PHIX_NOALLOC_MAX_ROWS 65536
 int phix_reduce_mass_energy_noalloc(const double* const* fields, int phys, const double* prm, const phix_grid_t* g,
                                     double* out, void* stream);

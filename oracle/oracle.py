@@ -19,6 +19,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_ORACLE = os.path.join(HERE, "liboracle.so")
+LIB_ORACLE_OMP = os.path.join(HERE, "liboracle_omp.so")  # same restatement, OpenMP loops
 LIB_REF = os.path.join(HERE, "_ref", "libphix_ref.so")
 
 BC_NONE, BC_PERIODIC, BC_NOFLUX, BC_FIXED = 0, 1, 2, 3
@@ -127,6 +128,11 @@ class Oracle:
             getattr(L, "or_mass" + sfx).restype = C.c_double
             getattr(L, "or_energy" + sfx).argtypes = [PP, C.c_int, C.POINTER(C.c_double), g]
             getattr(L, "or_energy" + sfx).restype = C.c_double
+
+    def threads(self) -> int:
+        """Host threads the library's loops run on (1 for liboracle.so)."""
+        f = getattr(self.lib, "or_threads", None)
+        return int(f()) if f else 1
 
     @staticmethod
     def _sfx(a):
@@ -275,7 +281,7 @@ def build(with_ref: bool | None = None, quiet: bool = True) -> None:
     """Compile the oracle (and, when the reference tree is present, oracle/_ref)."""
     import subprocess
     out = subprocess.DEVNULL if quiet else None
-    subprocess.run(["make", "-C", HERE, "liboracle.so"], check=True, stdout=out)
+    subprocess.run(["make", "-C", HERE, "liboracle.so", "liboracle_omp.so"], check=True, stdout=out)
     ref_src = os.environ.get("PHIX_REFERENCE_TREE", "/root/reference")
     if with_ref is None:
         with_ref = os.path.isdir(os.path.join(ref_src, "src"))

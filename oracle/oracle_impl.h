@@ -13,6 +13,19 @@
  * GPU solver's RK4 stage semantics.  Citations are to the reference project.
  */
 
+/* OpenMP build (liboracle_omp.so, -DOR_OMP): the per-cell loops and the
+ * whole-array stage combinations run on all host threads.  Every cell's
+ * arithmetic is unchanged, so both builds give the same bits. */
+#ifndef OR_PAR
+#ifdef OR_OMP
+#define OR_PAR _Pragma("omp parallel for schedule(static)")
+#define OR_PAR2 _Pragma("omp parallel for collapse(2) schedule(static)")
+#else
+#define OR_PAR
+#define OR_PAR2
+#endif
+#endif
+
 #define CAT_(a, b) a##b
 #define CAT(a, b) CAT_(a, b)
 #define FN(name) CAT(name, SFX)
@@ -43,6 +56,7 @@ static void FN(bc_face)(REAL* data, const or_grid_t* g, int axis, int type,
     if (axis == 0) { axis_stride = 1;       n_axis = g->n[0]; nf0 = sy; nf1 = sz; fs0 = sx; fs1 = sx * sy; }
     else if (axis == 1) { axis_stride = sx; n_axis = g->n[1]; nf0 = sx; nf1 = sz; fs0 = 1;  fs1 = sx * sy; }
     else { axis_stride = sx * sy;           n_axis = g->n[2]; nf0 = sx; nf1 = sy; fs0 = 1;  fs1 = sx; }
+    OR_PAR
     for (int t0 = 0; t0 < nf0; ++t0)
         for (int t1 = 0; t1 < nf1; ++t1) {
             long off = (long)t0 * fs0 + (long)t1 * fs1;
@@ -83,6 +97,15 @@ void FN(or_bc_apply)(REAL* data, const or_grid_t* g) {
  * Stencil accumulates.  Equation.cu:40-80 (lap) and :89-124 (grad).
  * ------------------------------------------------------------------------- */
 #define OR_LOOP_PHYS(g)                                                      \
+    int sx = (g)->n[0] + 2 * (g)->ghost, sy = (g)->n[1] + 2 * (g)->ghost;    \
+    int gh = (g)->ghost;                                                     \
+    OR_PAR2                                                                  \
+    for (int k = 0; k < (g)->n[2]; ++k)                                      \
+        for (int j = 0; j < (g)->n[1]; ++j)                                  \
+            for (int i = 0; i < (g)->n[0]; ++i)
+
+/* The same walk on one thread, for the order-dependent FP64 sums. */
+#define OR_LOOP_PHYS_SEQ(g)                                                  \
     int sx = (g)->n[0] + 2 * (g)->ghost, sy = (g)->n[1] + 2 * (g)->ghost;    \
     int gh = (g)->ghost;                                                     \
     for (int k = 0; k < (g)->n[2]; ++k)                                      \
@@ -145,6 +168,7 @@ void FN(or_grad_acc)(REAL* rhs, const REAL* src, double coeff, int axis, const o
 /* dst[i] = fma(coeff, src[i], dst[i]) over n elements (kernel_axpy,
  * Solver.cu:30-35, as the contracted device build computes it). */
 void FN(or_axpy)(REAL* dst, const REAL* src, double coeff, long n, int mode) {
+    OR_PAR
     for (long i = 0; i < n; ++i) dst[i] = FN(madd)(mode, (REAL)coeff, src[i], dst[i]);
 }
 
@@ -216,6 +240,11 @@ void FN(or_mul_acc)(REAL* rhs, const REAL* s1, const REAL* s2, double coeff, con
  *     CH   : [M, kappa, rho, ca, cb]
  *     CHAC : [M, L, kappa_c, kappa_eta, lambda]
  * ------------------------------------------------------------------------- */
+static void FN(zero)(REAL* a, long n) {
+    OR_PAR
+    for (long i = 0; i < n; ++i) a[i] = 0;
+}
+
 static long FN(stored)(const or_grid_t* g) {
     return (long)(g->n[0] + 2 * g->ghost) * (g->n[1] + 2 * g->ghost) * (g->n[2] + 2 * g->ghost);
 }
@@ -225,13 +254,13 @@ void FN(or_rhs)(REAL** rhs, REAL** u, int phys, const double* prm,
     long S = FN(stored)(g);
     if (phys == OR_PHYS_AC) {
         /* L*kappa*lap(phi) + L*pw(phi, p - p^3) */
-        memset(rhs[0], 0, sizeof(REAL) * S);
+        FN(zero)(rhs[0], S);
         FN(or_lap_acc)(rhs[0], u[0], prm[0] * prm[1], g);
         FN(or_pw_acc)(rhs[0], u[0], 0, prm[0], OR_PW_AC, prm, g);
     } else if (phys == OR_PHYS_CH) {
         /* M*lap(pw(c, f') - kappa*lap(c), bcs) */
-        memset(rhs[0], 0, sizeof(REAL) * S);
-        memset(scratch, 0, sizeof(REAL) * S);
+        FN(zero)(rhs[0], S);
+        FN(zero)(scratch, S);
         FN(or_pw_acc)(scratch, u[0], 0, 1.0, OR_PW_DW, prm, g);
         FN(or_lap_acc)(scratch, u[0], -prm[1], g);
         FN(or_bc_apply)(scratch, g);
@@ -239,13 +268,13 @@ void FN(or_rhs)(REAL** rhs, REAL** u, int phys, const double* prm,
     } else if (phys == OR_PHYS_CHAC) {
         /* c  : M*lap(pw(c, eta, f_c) - kappa_c*lap(c), bcs)
          * eta: (-L)*pw(eta, c, f_eta) + (L*kappa_eta)*lap(eta) */
-        memset(rhs[0], 0, sizeof(REAL) * S);
-        memset(scratch, 0, sizeof(REAL) * S);
+        FN(zero)(rhs[0], S);
+        FN(zero)(scratch, S);
         FN(or_pw_acc)(scratch, u[0], u[1], 1.0, OR_PW_CHAC_C, prm, g);
         FN(or_lap_acc)(scratch, u[0], -prm[2], g);
         FN(or_bc_apply)(scratch, g);
         FN(or_lap_acc)(rhs[0], scratch, prm[0], g);
-        memset(rhs[1], 0, sizeof(REAL) * S);
+        FN(zero)(rhs[1], S);
         FN(or_pw_acc)(rhs[1], u[1], u[0], -prm[1], OR_PW_CHAC_E, prm, g);
         FN(or_lap_acc)(rhs[1], u[1], prm[1] * prm[3], g);
     }
@@ -284,8 +313,10 @@ int FN(or_advance)(REAL** u, int phys, const double* prm, int scheme,
         for (int f = 0; f < nf; ++f) FN(or_bc_apply)(u[f], g);
         if (scheme == OR_EULER) {
             FN(or_rhs)(k1, u, phys, prm, g, scratch);
-            for (int f = 0; f < nf; ++f)
+            for (int f = 0; f < nf; ++f) {
+                OR_PAR
                 for (long i = 0; i < S; ++i) u[f][i] = FN(madd)(mode, dtr, k1[f][i], u[f][i]);
+            }
             continue;
         }
         FN(or_rhs)(k1, u, phys, prm, g, scratch);
@@ -294,17 +325,20 @@ int FN(or_advance)(REAL** u, int phys, const double* prm, int scheme,
         REAL as[3] = {dt2, dt2, dtr};
         for (int st = 0; st < 3; ++st) {
             for (int f = 0; f < nf; ++f) {
+                OR_PAR
                 for (long i = 0; i < S; ++i) tmp[f][i] = FN(madd)(mode, as[st], ks[st][f][i], u[f][i]);
                 FN(or_bc_apply)(tmp[f], g);
             }
             FN(or_rhs)(kn[st], tmp, phys, prm, g, scratch);
         }
-        for (int f = 0; f < nf; ++f)
+        for (int f = 0; f < nf; ++f) {
+            OR_PAR
             for (long i = 0; i < S; ++i) {
                 REAL a = (k1[f][i] + (REAL)2 * k2[f][i]) + (REAL)2 * k3[f][i];
                 a = a + k4[f][i];
                 u[f][i] = FN(madd)(mode, dt6, a, u[f][i]);
             }
+        }
     }
     free(buf);
     return 0;
@@ -394,12 +428,13 @@ int FN(or_advance_ch_multistep)(REAL* c, REAL* mu, const double* prm, double dt,
     if (!rhs) return -1;
     for (int s = 0; s < nsteps; ++s) {
         FN(or_bc_apply)(c, g);
-        memset(mu, 0, sizeof(REAL) * S);
+        FN(zero)(mu, S);
         FN(or_pw_acc)(mu, c, 0, 1.0, OR_PW_DW, prm, g);
         FN(or_lap_acc)(mu, c, -prm[1], g);
         FN(or_bc_apply)(mu, g);
-        memset(rhs, 0, sizeof(REAL) * S);
+        FN(zero)(rhs, S);
         FN(or_lap_acc)(rhs, mu, prm[0], g);
+        OR_PAR
         for (long i = 0; i < S; ++i) c[i] = FN(madd)(mode, (REAL)dt, rhs[i], c[i]);
     }
     free(rhs);
@@ -422,7 +457,7 @@ static double FN(dvol)(const or_grid_t* g) {
 
 double FN(or_mass)(const REAL* u, const or_grid_t* g) {
     double s = 0.0;
-    OR_LOOP_PHYS(g) { s += (double)u[OR_IDX(i, j, k)]; }
+    OR_LOOP_PHYS_SEQ(g) { s += (double)u[OR_IDX(i, j, k)]; }
     return s * FN(dvol)(g);
 }
 
@@ -442,7 +477,7 @@ double FN(or_energy)(REAL** u_in, int phys, const double* prm, const or_grid_t* 
     else if (phys == OR_PHYS_CH) kap[0] = prm[1];
     else { kap[0] = prm[2]; kap[1] = prm[3]; }
     double tot = 0.0;
-    OR_LOOP_PHYS(g) {
+    OR_LOOP_PHYS_SEQ(g) {
         long c = OR_IDX(i, j, k);
         long off[3] = {1, sx, (long)sx * sy};
         double fb;
@@ -472,6 +507,7 @@ double FN(or_energy)(REAL** u_in, int phys, const double* prm, const or_grid_t* 
 }
 
 #undef OR_LOOP_PHYS
+#undef OR_LOOP_PHYS_SEQ
 #undef OR_IDX
 #undef FN
 #undef CAT

@@ -3,7 +3,9 @@
  *
  * TEST INFRASTRUCTURE ONLY: a plain-C restatement of the reference algorithm
  * used to check the sm_100a kernels.  The product never links or calls it.
- * Build: oracle/Makefile -> oracle/liboracle.so (gcc -O2 -ffp-contract=off).
+ * Build: oracle/Makefile -> oracle/liboracle.so (gcc -O2 -ffp-contract=off), and
+ * oracle/liboracle_omp.so (the same source with OpenMP on every per-cell loop:
+ * the timed CPU baseline on all host cores; identical bits).
  *
  * Pinning: tests/test_oracle_pin.py checks this restatement, in fma_mode 0,
  * bit for bit against the reference's own CPU path compiled from its sources
@@ -53,3 +55,11 @@ typedef struct {
 #undef FMA
 
 int or_abi_version(void) { return 1; }
+
+#ifdef OR_OMP
+#include <omp.h>
+/* Host threads the OpenMP build runs its loops on. */
+int or_threads(void) { return omp_get_max_threads(); }
+#else
+int or_threads(void) { return 1; }
+#endif

@@ -18,7 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libphix_b200.so")
 
-OK, ERR_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_NONFINITE = 0, -1, -2, -3, -4
+OK, ERR_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_NONFINITE, ERR_TIMEOUT = 0, -1, -2, -3, -4, -5
 BC_NONE, BC_PERIODIC, BC_NOFLUX, BC_FIXED = 0, 1, 2, 3
 PHYS_AC, PHYS_CH, PHYS_CHAC = 0, 1, 2
 EULER, RK4, MULTISTEP = 0, 1, 2
@@ -138,6 +138,8 @@ def lib() -> C.CDLL:
         "phix_surrogate_grad": ([vp, vp, vp, C.c_int, P, vp], C.c_int),
         "phix_surrogate_adam": ([vp, vp, C.c_float, vp], C.c_int),
         "phix_surrogate_grad_ptr": ([vp], C.c_void_p),
+        "phix_surrogate_status": ([vp, vp], C.c_int),
+        "phix_wait_selftest": ([C.c_int, C.c_double, vp], C.c_int),
         "phix_plane_gather": ([vp, vp, C.c_int, C.c_int, C.c_int, vp], C.c_int),
         "phix_plane_scatter": ([vp, vp, C.c_int, C.c_int, C.c_int, vp], C.c_int),
         "phix_stepper_diagnostics": ([vp, P], C.c_int),
@@ -466,6 +468,11 @@ class Surrogate:
 
     def grad_ptr(self) -> int:
         return lib().phix_surrogate_grad_ptr(self.h)
+
+    def status(self, stream=None):
+        """Raise PhixError (code ERR_TIMEOUT) if a bounded tensor-core wait of
+        this surrogate's kernels gave up since the last check; clears it."""
+        check(lib().phix_surrogate_status(self.h, _stream(stream)))
 
     def adam(self, lr: float, grads=None, stream=None):
         gp = C.c_void_p(grads.data_ptr()) if grads is not None else None

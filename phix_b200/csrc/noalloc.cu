@@ -2,11 +2,16 @@
 //
 // phix_reduce_mass_energy obtains its scratch (per-block partial sums) with
 // cudaMallocAsync on every call.  Some callers cannot allocate device memory:
-// code that runs while a CUDA graph is being captured by someone else, hosts
-// whose device memory is owned and pre-reserved by another runtime or a
-// custom allocator, and embedded or real-time loops that forbid allocation
+// hosts whose device memory is owned and pre-reserved by another runtime or a
+// custom allocator (an allocation from this library would fail or break that
+// owner's accounting), and embedded or real-time loops that forbid allocation
 // after start-up.  phix_reduce_mass_energy_noalloc gives them the same
 // diagnostics with the scratch in a file-scope device array instead.
+//
+// The call is synchronous: it copies the result to the host and waits for
+// `stream`.  So it must not be made on a stream under capture, and with
+// stream = NULL (the legacy default stream) no global-mode capture may be
+// active in the process.
 //
 // Scratch: one (mass, energy, non-finite count) triple per physical row of
 // the grid (n[1] * n[2] rows) plus the three result slots, in
@@ -16,6 +21,11 @@
 // but all calls share the one array: calls that overlap on the GPU (on
 // different streams, or from different host threads) race and must be
 // serialised by the caller.
+//
+// The array's device address is looked up once per device (the first call
+// there) and kept for the life of the process.  It belongs to that device's
+// primary context: a process that destroys the context (cudaDeviceReset) must
+// not call this entry point on that device afterwards.
 #include <cmath>
 #include <mutex>
 

@@ -1476,7 +1476,7 @@ int phix_surrogate_grad(phix_surrogate_t* s, const double* c, const double* c_ne
     int herr = 0;
     PHIX_TRY_CUDA(cudaMemcpyAsync(&herr, s->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     PHIX_TRY_CUDA(cudaStreamSynchronize(st));
-    if (herr) { set_error("surrogate: a tensor-core wait timed out"); return PHIX_ERR_CUDA; }
+    if (herr) { set_error("surrogate: a tensor-core wait timed out"); return PHIX_ERR_TIMEOUT; }
     double tot = 0.0;
     for (double v : lp) tot += v;
     if (loss) *loss = tot / (double)N;
@@ -1500,6 +1500,19 @@ int phix_surrogate_adam(phix_surrogate_t* s, const float* grads, float lr, void*
     return sg_pack(s, st);
 }
 
+// Reads and clears the surrogate's device error flag (set by a kernel whose
+// bounded tensor-core wait gave up); synchronous on `stream`.
+int phix_surrogate_status(phix_surrogate_t* s, void* stream) {
+    if (!s) { set_error("surrogate_status: NULL surrogate"); return PHIX_ERR_ARG; }
+    cudaStream_t st = (cudaStream_t)stream;
+    int herr = 0;
+    PHIX_TRY_CUDA(cudaMemcpyAsync(&herr, s->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PHIX_TRY_CUDA(cudaMemsetAsync(s->err, 0, sizeof(int), st));
+    PHIX_TRY_CUDA(cudaStreamSynchronize(st));
+    if (herr) { set_error("surrogate: a tensor-core wait timed out"); return PHIX_ERR_TIMEOUT; }
+    return PHIX_OK;
+}
+
 // Device pointer of the internal FP32 gradient vector (NPARAM floats).
 float* phix_surrogate_grad_ptr(phix_surrogate_t* s) { return s ? s->grads : nullptr; }
 
@@ -1514,6 +1527,37 @@ int phix_plane_scatter(const double* plane, double* stored, int H, int W, int gh
     if (!stored || !plane || H < 1 || W < 1 || ghost < 0) { set_error("plane_scatter: bad argument"); return PHIX_ERR_ARG; }
     scatter_plane<<<dim3((W + 255) / 256, H), 256, 0, (cudaStream_t)stream>>>(plane, stored, H, W, ghost);
     PHIX_LAUNCH_CHECK("scatter_plane");
+    return PHIX_OK;
+}
+
+// Self-test of the bounded mbarrier wait of the tensor-core kernels: one
+// thread initialises a barrier of count 1, arrives on it when `arrive`, and
+// waits for its first phase with a wall-clock limit.  With no arrival the wait
+// gives up after limit_ns and the kernel records that in the flag and
+// returns, as the tensor-core kernels do, leaving the context usable.
+__global__ void wait_selftest(int arrive, unsigned long long limit_ns, int* flag) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    tc::mbar_init(&bar, 1);
+    if (arrive) tc::mbar_arrive(&bar);
+    if (!tc::mbar_wait_bounded(&bar, 0, limit_ns)) atomicExch(flag, 1);
+}
+
+static __device__ int g_wait_selftest_flag;
+
+int phix_wait_selftest(int arrive, double limit_s, void* stream) {
+    if (!(limit_s > 0.0 && limit_s <= 2.0)) { set_error("wait_selftest: limit %g s outside (0, 2]", limit_s); return PHIX_ERR_ARG; }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int zero = 0;
+    PHIX_TRY_CUDA(cudaMemcpyToSymbolAsync(g_wait_selftest_flag, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st));
+    int* flag = nullptr;  // device address of the flag (the symbol is a host-side stand-in)
+    PHIX_TRY_CUDA(cudaGetSymbolAddress((void**)&flag, g_wait_selftest_flag));
+    wait_selftest<<<1, 32, 0, st>>>(arrive, (unsigned long long)(limit_s * 1e9), flag);
+    PHIX_LAUNCH_CHECK("wait_selftest");
+    int herr = 0;
+    PHIX_TRY_CUDA(cudaMemcpyFromSymbolAsync(&herr, g_wait_selftest_flag, sizeof(int), 0, cudaMemcpyDeviceToHost, st));
+    PHIX_TRY_CUDA(cudaStreamSynchronize(st));
+    if (herr) { set_error("wait_selftest: the bounded wait gave up after %g s", limit_s); return PHIX_ERR_TIMEOUT; }
     return PHIX_OK;
 }
 

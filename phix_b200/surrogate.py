@@ -87,11 +87,24 @@ def generate(seeds, nsteps: int, every: int = STEPS_PER_CALL, n: int = N, precis
 
 def shard_seeds(seeds, rank: int, world: int):
     """Data-parallel training: rank r generates and trains on seeds r,
-    r+world, ...; every rank gets the same number (the remainder is dropped),
-    so all ranks take the same number of gradient all-reduces."""
-    seeds = list(seeds)
-    per = len(seeds) // world
-    return seeds[rank::world][:per]
+    r+world, ...  Every seed is assigned, so shards differ in length by at
+    most one; train() pads the shorter shards' schedules with zero-weight
+    updates so that all ranks take the same number of gradient all-reduces."""
+    return list(seeds)[rank::world]
+
+
+def dp_update_counts(shard_sizes, ns: int, chunk: int, batch: int, epochs: int):
+    """Adam updates each rank's shard yields in train(): per chunk of
+    `chunk` trajectories of `ns` snapshots, `epochs` passes over the chunk's
+    (ns - 1) * T pairs in whole batches."""
+    counts = []
+    for size in shard_sizes:
+        u = 0
+        for start in range(0, size, chunk):
+            t = min(chunk, size - start)
+            u += epochs * ((t * (ns - 1)) // batch)
+        counts.append(u)
+    return counts
 
 
 def allreduce_mean_(t, group=None):
@@ -100,6 +113,20 @@ def allreduce_mean_(t, group=None):
     import torch.distributed as dist
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     t.div_(dist.get_world_size(group))
+    return t
+
+
+def allreduce_active_mean_(t, active: bool, n_active: int, group=None):
+    """In-place mean over the ranks that still have a batch: a rank whose
+    shard is used up (`active` False) contributes zeros but still takes part
+    in the all-reduce, so every rank issues the same collectives and applies
+    the same averaged gradient.  `n_active` (>= 1) is the number of active
+    ranks, known on every rank from dp_update_counts."""
+    import torch.distributed as dist
+    if not active:
+        t.zero_()
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    t.div_(n_active)
     return t
 
 
@@ -130,13 +157,20 @@ def train(seeds, nsteps: int = 40000, every: int = STEPS_PER_CALL, batch: int = 
     log = TrainLog()
     seeds = list(seeds)
     grads = None
+    ns = nsteps // every + 1
+    counts = dp_update_counts([len(seeds)], ns, chunk, batch, epochs)
     if distributed:
         import torch.distributed as dist
-        seeds = shard_seeds(seeds, dist.get_rank(), dist.get_world_size())
+        world = dist.get_world_size()
+        shards = [shard_seeds(seeds, r, world) for r in range(world)]
+        counts = dp_update_counts([len(x) for x in shards], ns, chunk, batch, epochs)
+        seeds = shards[dist.get_rank()]
         grads = torch.as_tensor(_DeviceVector(sg.grad_ptr(), sg.nparams), device="cuda")
     rng = np.random.default_rng(shuffle_seed)
-    ns = nsteps // every + 1
-    total = max(1, (len(seeds) * (ns - 1) * epochs) // batch)
+    total = max(1, max(counts))  # the same learning-rate schedule on every rank
+
+    def n_active(u):
+        return sum(1 for c in counts if c > u)
     for start in range(0, len(seeds), chunk):
         t0 = time.perf_counter()
         data = generate(seeds[start:start + chunk], nsteps, every, n)
@@ -153,7 +187,7 @@ def train(seeds, nsteps: int = 40000, every: int = STEPS_PER_CALL, batch: int = 
                 nxt = data[ti, si + 1].contiguous()
                 loss = sg.grad(a, nxt)
                 if grads is not None:
-                    allreduce_mean_(grads)
+                    allreduce_active_mean_(grads, True, n_active(log.updates))
                 rate = lr * (lr_final / lr) ** min(1.0, log.updates / total)
                 sg.adam(rate)
                 log.updates += 1
@@ -165,6 +199,12 @@ def train(seeds, nsteps: int = 40000, every: int = STEPS_PER_CALL, batch: int = 
         torch.cuda.synchronize()
         log.seconds_train += time.perf_counter() - t0
         del data
+    # a shorter shard's rank keeps taking part in the all-reduces (with a
+    # zero gradient) and applies the same Adam steps until every rank is done
+    while grads is not None and log.updates < total:
+        allreduce_active_mean_(grads, False, n_active(log.updates))
+        sg.adam(lr * (lr_final / lr) ** min(1.0, log.updates / total))
+        log.updates += 1
     p, _ = sg.get_params()
     sg.close()
     return p, log

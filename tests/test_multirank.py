@@ -97,12 +97,74 @@ def test_batch_instances_partitioned_across_two_ranks():
     assert max(loads) - min(loads) <= 1024 * 1024  # within the largest instance
 
 
-def test_seed_shards_are_disjoint_and_equal_sized():
-    from phix_b200.surrogate import shard_seeds
+def test_seed_shards_cover_every_seed():
+    from phix_b200.surrogate import dp_update_counts, shard_seeds
     shards = [shard_seeds(range(100, 300), r, 3) for r in range(3)]
-    assert len({len(x) for x in shards}) == 1
-    flat = [s for x in shards for s in x]
-    assert len(flat) == len(set(flat)) == 198
+    assert sorted(s for x in shards for s in x) == list(range(100, 300))
+    assert sorted(len(x) for x in shards) == [66, 67, 67]
+    # 801 snapshots, chunks of 25 trajectories, batch 16, 2 epochs
+    counts = dp_update_counts([len(x) for x in shards], 801, 25, 16, 2)
+    assert counts[0] == counts[1] > counts[2]
+    assert counts[2] == 2 * ((25 * 800) // 16) * 2 + 2 * ((16 * 800) // 16)
+
+
+def _dp_active_worker(rank, world, port, out):
+    _init(rank, world, port)
+    try:
+        from phix_b200 import surrogate as S
+        g = torch.full((5,), float(rank + 1), dtype=torch.float64)
+        S.allreduce_active_mean_(g, active=(rank == 0), n_active=1)  # rank 1's shard is used up
+        both = torch.full((5,), float(rank + 1), dtype=torch.float64)
+        S.allreduce_active_mean_(both, active=True, n_active=2)
+        got = [None] * world
+        dist.all_gather_object(got, (g.numpy().copy(), both.numpy().copy()))
+        if rank == 0:
+            out.put(got)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_padded_update_takes_only_the_active_ranks_gradient():
+    got = _run(_dp_active_worker)
+    for g, both in got:  # every rank applies the same averaged gradient
+        assert np.array_equal(g, np.full(5, 1.0))
+        assert np.array_equal(both, np.full(5, 1.5))
+
+
+def _bench_worker(rank, world, port, out):
+    _init(rank, world, port)
+    try:
+        import bench
+        env = {"WORLD_SIZE": str(world), "RANK": str(rank)}
+        w = bench.resolve_world(world, env)
+        # rank r timed (r + 1) * 10 ms and advanced (r + 1) * 1000 cells per time step
+        total_ms, cells, e2e_ms = bench.combine_over_ranks(10.0 * (rank + 1), 1000.0 * (rank + 1),
+                                                           3.0 + rank, torch.device("cpu"), w)
+        job = bench.job_summary(w, 4, 100, total_ms, cells)
+        if rank == 0:
+            out.put((job, e2e_ms))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_rank_logic_two_ranks():
+    job, e2e_ms = _run(_bench_worker)
+    assert job["n_gpus"] == 2
+    assert job["ms_per_step"] == 20.0 / 4  # the slowest rank
+    assert job["value"] == 3000.0 * 100 * 4 / 0.020  # cells of both ranks
+    assert e2e_ms == 4.0
+
+
+def test_bench_world_size_must_match_gpus():
+    import bench
+    assert bench.resolve_world(1, {}) == 1
+    assert bench.resolve_world(4, {}) == 1  # main() launches the ranks itself
+    assert bench.resolve_world(2, {"WORLD_SIZE": "2"}) == 2
+    with pytest.raises(SystemExit):
+        bench.resolve_world(4, {"WORLD_SIZE": "2"})
+    cmd = bench.launcher_command(["--gpus", "2", "--steps", "3"], 2, 29512)
+    assert "--nproc-per-node=2" in cmd and "--master-addr=127.0.0.1" in cmd
+    assert cmd[-4:] == ["--gpus", "2", "--steps", "3"]
 
 
 def test_data_parallel_gradient_average_equals_full_batch():

@@ -46,14 +46,18 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda):
                                         px.BC_PERIODIC)), 2),
     ]
     for seed, (phys, prm, g, nf) in enumerate(cases):
-        # the larger grid first, then a smaller one: stale rows of the first
-        # call sit beyond the second call's rows and must not be summed
+        # two calls in a row on the same grid with different fields: the
+        # second must not see the first call's rows (stale rows beyond a
+        # smaller grid are covered by test_noalloc_second_call_on_smaller_grid)
         for call in range(2):
             fields = _fields(10 * seed + call, g, nf)
             want = px.reduce_mass_energy(fields, phys, prm, g)
             got = _call_noalloc(fields, phys, prm, g)
             for a, b in zip(got, want):
                 assert abs(a - b) <= TOL * abs(b), (phys, call, a, b)
+            # the Python binding of the same entry point marshals the same call
+            wrapped = px.reduce_mass_energy_noalloc(fields, phys, prm, g)
+            assert wrapped == got
 
 
 @pytest.mark.gpu
@@ -66,6 +70,30 @@ def test_noalloc_second_call_on_smaller_grid(cuda):
         got = _call_noalloc(fields, px.PHYS_CH, prm, g)
         for a, b in zip(got, want):
             assert abs(a - b) <= TOL * abs(b)
+
+
+@pytest.mark.gpu
+def test_noalloc_flags_non_finite_cells_then_recovers(cuda):
+    """One NaN physical cell gives PHIX_ERR_NONFINITE; the next clean call on
+    the same (shared) scratch matches the allocating entry point again."""
+    prm = [1.0, 0.5, 1.0, 0.0, 1.0]
+    g = px.make_grid((96, 80))
+    bad = _fields(5, g, 1)
+    bad[0][1, 40, 30] = float("nan")  # a physical cell: z plane 1 of the 2-D stored array (ghost 1)
+    lib = px.lib()
+    ptrs = (C.c_void_p * 1)(bad[0].data_ptr())
+    prmc = (C.c_double * 8)(*(prm + [0.0] * 3))
+    out = (C.c_double * 2)()
+    rc = lib.phix_reduce_mass_energy_noalloc(ptrs, px.PHYS_CH, prmc, C.byref(g), out, None)
+    assert rc == px.ERR_NONFINITE
+    assert b"non-finite" in lib.phix_last_error()
+    with pytest.raises(px.PhixError):
+        px.reduce_mass_energy_noalloc(bad, px.PHYS_CH, prm, g)
+    clean = _fields(6, g, 1)
+    want = px.reduce_mass_energy(clean, px.PHYS_CH, prm, g)
+    got = _call_noalloc(clean, px.PHYS_CH, prm, g)
+    for a, b in zip(got, want):
+        assert abs(a - b) <= TOL * abs(b)
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
