@@ -187,6 +187,14 @@ TRAFFIC = {
     ("ch2d_ms", "f64", "step_pair_ms"): 8.45e6,  # CH 1024^2 multi-step Euler
 }
 
+# Lane operations (fma = 2) of one RK4 cell-update in step2d_pair.cuh, on the
+# tile's own cells: per stage the mu pass (Laplacian 8, f' 7, mu 4 = 19) and
+# the k pass (Laplacian 8, k 2, y 2, RK4 sum 0 / 2 / 2; final: sum 1, update 2):
+# 4 x 19 + 12 + 14 + 14 + 13 = 129.  FP32's final pass forms dt/6 * sum (1)
+# and the compensated two-sum update (10 add/sub) in place of the fma (2).
+PAIR_FLOPS_F64 = 129
+PAIR_FLOPS_F32 = 138
+
 # step tiles 6 and up are the pair kernels (include/phix_b200.h, phix_stepper_set_tiles)
 FIRST_PAIR_TILE = 6
 
@@ -194,6 +202,8 @@ FIRST_PAIR_TILE = 6
 def dominant_kernel(px, g, phys, scheme, lps, fused, tile):
     """Name of the kernel that takes the time step (the key of TRAFFIC)."""
     periodic_ch = phys == px.PHYS_CH and g.dim == 2 and all(g.bc_type[i] == px.BC_PERIODIC for i in range(4))
+    if g.dim == 3:
+        return "stage2_march3d" if lps == 2 else "stage_march3d"
     if scheme == px.MULTISTEP:
         return "step_pair_ms" if fused else "stage_box"
     if lps == 1 and scheme == px.RK4 and fused:
@@ -440,6 +450,22 @@ def bench_ours(args):
     if args.workload == "ch2d" and args.n != 1024:
         workload = workload.replace("1024^2", f"{args.n}^2")
 
+    # arithmetic-pipe roofline of the CH pair kernel (L2-resident at 1024^2):
+    # lane operations (fma = 2) per cell-update counted from step2d_pair.cuh
+    # on the tile's own cells, over the measured FMA peak of this GPU
+    pipe = None
+    if args.workload == "ch2d" and getattr(run, "kernel", "") == "step_pair":
+        fp64 = run.prec == px.F64
+        flops = PAIR_FLOPS_F64 if fp64 else PAIR_FLOPS_F32
+        peak_t = px.measure_fma_peak(px.F64) if fp64 else px.measure_fma_peak(px.F32, packed=True)
+        ach_t = flops * run.cells * K / (ms_per_step / 1e3) / 1e12
+        pipe = {"bound": "fp64" if fp64 else "fp32", "achieved": ach_t, "peak": peak_t, "unit": "TFLOP/s",
+                "frac": ach_t / peak_t, "flops_per_cell_update": flops,
+                "note": "lane operations per cell-update on the tile's own cells (fma = 2), counted from the "
+                        "kernel source; the halo recompute of the 4-stage tile adds about 43 % more; peak = "
+                        "phix_measure_fma_peak on this GPU (" + ("FP64 FMA" if fp64 else "packed f32x2 FMA") +
+                        " chains on every SM)"}
+
     if args.no_e2e:
         run.close()
         if rank == 0:
@@ -527,6 +553,7 @@ def bench_ours(args):
                                  f"one time step ({run.lps} launch{'es' if run.lps > 1 else ''} per time step); "
                                  f"peak {peak_kind} (MEASURED_PEAKS.json hbm_gbs); traffic = ncu DRAM bytes per "
                                  f"launch of the dominant kernel (bytes, cold L2)"},
+            "roofline_pipe": pipe,
             "hbm_gbs_effective": achieved,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": run.io_bytes,

@@ -27,7 +27,9 @@ namespace phix {
 // (Solver.cu:317-340 with Cahn-Hillard_double-well.cu:84-106): mu (STEADY) is
 // the smem mu of the tile, written out as a field; c (TRANSIENT) gets the
 // Euler update from M*lap(mu).
-enum : int { MODE_K = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2, MODE_MULTISTEP = 3 };
+// MODE_RK4_STEP (C++ DSL launches only): the whole RK4 step in one launch
+// (the pair kernel of step2d_pair.cuh), where the grid and term form allow.
+enum : int { MODE_K = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2, MODE_MULTISTEP = 3, MODE_RK4_STEP = 4 };
 
 template <typename T>
 struct StageArgs {

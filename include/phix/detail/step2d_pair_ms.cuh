@@ -40,39 +40,6 @@ struct MsPair {
     static constexpr int MINB = MINB1 < 1 ? 1 : MINB1;
 };
 
-// mu and the right-hand side of a pair through the policy (lane by lane).
-template <typename T, class Pol>
-struct PairPolicy {
-    using V = typename PairOf<T>::V;
-    __device__ static __forceinline__ V mu(const StageArgs<T>& S, const Pol& pol, V c, V lap, V) {
-        return V{pol.mu(S, c.x, lap.x, (T)0), pol.mu(S, c.y, lap.y, (T)0)};
-    }
-    __device__ static __forceinline__ V rhs(const StageArgs<T>& S, const Pol& pol, V lapmu, V c) {
-        T kx[2], ky[2];
-        pol.rhs(S, lapmu.x, c.x, (T)0, (T)0, (T)0, kx);
-        pol.rhs(S, lapmu.y, c.y, (T)0, (T)0, (T)0, ky);
-        return V{kx[0], ky[0]};
-    }
-};
-
-// PolCH: the packed forms of step_pair (pair_mu_pass, pair_k_pass).
-template <typename T>
-struct PairPolicy<T, PolCH> {
-    using V = typename PairOf<T>::V;
-    __device__ static __forceinline__ V mu(const StageArgs<T>& S, const PolCH&, V c, V lap, V v2) {
-        const V two_rho = p_splat(S.p[2]), ca = p_splat(S.p[3]), cb = p_splat(S.p[4]);
-        const V mk = p_splat(S.p[1]), one = p_splat((T)1), zero = p_splat((T)0);
-        // f'(c) = (two_rho (c - ca)) (c - cb) ((2c - ca) - cb)   (f_dw)
-        const V fa = p_mul(p_mul(two_rho, p_sub(c, ca)), p_sub(c, cb));
-        const V fd = p_mul(fa, p_sub(p_sub(v2, ca), cb));
-        // mu = (-kappa) lap + (1 f' + 0)   (PolCH::mu)
-        return p_fma(mk, lap, p_fma(one, fd, zero));
-    }
-    __device__ static __forceinline__ V rhs(const StageArgs<T>& S, const PolCH&, V lapmu, V) {
-        return p_fma(p_splat(S.p[0]), lapmu, p_splat((T)0));
-    }
-};
-
 template <typename T, class Pol, int TX, int TY, int NRP>
 __device__ __forceinline__ void ms_pair_tile(const StageArgs<T>& S, const Pol& pol, T* __restrict__ sm, int x0,
                                              int y0) {

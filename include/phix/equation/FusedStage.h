@@ -6,6 +6,7 @@
 // op_i is the Laplacian of y or the term's functor of y; y is the stage state.
 
 #include "phix/detail/stage.cuh"
+#include "phix/detail/step2d_pair.cuh"
 
 namespace PhiX {
 namespace fuse {
@@ -23,6 +24,7 @@ struct StageSpec {
     int dim = 2;
     int mode = phix::MODE_K;             // phix::MODE_*
     phix::StageArgs<double> A{};         // layout, pointers, a, dtf, i2
+    double dt_half = 0.0, dt_full = 0.0;  // MODE_RK4_STEP: the stage-state factors dt/2 and dt
 };
 
 // Stage policy evaluating the term program with the user's functor F.

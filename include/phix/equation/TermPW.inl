@@ -68,6 +68,30 @@ struct PwKernelsImpl final : fuse::PwKernels {
             pol.c[i] = s.c[i];
         }
         const phix::StageArgs<double>& A = s.A;
+        if constexpr (MODE == phix::MODE_RK4_STEP) {
+            // the whole RK4 step as one launch of the pair kernel (64x28 tiles,
+            // 8 row blocks: the FP64 shape the C ABI picks at 1024^2)
+            if constexpr (DIM == 2 && PAT == fuse::PATTERN_COMPOSITE) {
+                if (!phix::step_pair_supported(A.L, 2)) return PHIX_ERR_UNSUPPORTED;
+                using G = phix::StepPair<double, 64, 28, 8>;
+                phix::StepArgs<double> B;
+                B.S = A;
+                B.dt2 = s.dt_half;
+                B.dt = s.dt_full;
+                dim3 grid((A.L.n[0] + 63) / 64, (A.L.n[1] + 27) / 28, 1);
+                phix::step_pair<double, Pol, 64, 28, 8><<<grid, G::NT, G::smem_bytes(), st>>>(B, pol);
+                count_user_launch();
+                return cudaGetLastError() == cudaSuccess ? PHIX_OK : PHIX_ERR_CUDA;
+            } else {
+                return PHIX_ERR_UNSUPPORTED;
+            }
+        } else {
+            return run_stage<PAT, DIM, MODE>(pol, s, st);
+        }
+    }
+    template <int PAT, int DIM, int MODE, class Pol>
+    int run_stage(const Pol& pol, const fuse::StageSpec& s, cudaStream_t st) const {
+        const phix::StageArgs<double>& A = s.A;
         if constexpr (DIM == 2 && MODE == phix::MODE_MULTISTEP && PAT == fuse::PATTERN_COMPOSITE) {
             if (phix::step_pair_supported(A.L, 2)) {
                 // the multi-step form on four periodic sides: the pair kernel
@@ -102,6 +126,9 @@ struct PwKernelsImpl final : fuse::PwKernels {
             case phix::MODE_MULTISTEP:
                 if (PAT == fuse::PATTERN_COMPOSITE && DIM < 3) return run<PAT, DIM, phix::MODE_MULTISTEP>(s, st);
                 return PHIX_ERR_UNSUPPORTED;
+            case phix::MODE_RK4_STEP:
+                if (PAT == fuse::PATTERN_COMPOSITE && DIM == 2) return run<PAT, DIM, phix::MODE_RK4_STEP>(s, st);
+                return PHIX_ERR_UNSUPPORTED;
         }
         return PHIX_ERR_ARG;
     }
@@ -123,6 +150,13 @@ struct PwKernelsImpl final : fuse::PwKernels {
         return e == cudaSuccess ? PHIX_OK : PHIX_ERR_CUDA;
     }
     int prepare(int dim) const override {
+        if (dim == 2) {  // the one-launch RK4 step's shared memory (99 KB)
+            using Pol = fuse::PolUser<F, fuse::PATTERN_COMPOSITE>;
+            using G = phix::StepPair<double, 64, 28, 8>;
+            cudaError_t e = cudaFuncSetAttribute(phix::step_pair<double, Pol, 64, 28, 8>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes());
+            return e == cudaSuccess ? PHIX_OK : PHIX_ERR_CUDA;
+        }
         if (dim != 3) return PHIX_OK;
         int rc = PHIX_OK;
         if (!rc) rc = prepare_march<fuse::PATTERN_FLAT, phix::MODE_K>();

@@ -146,11 +146,20 @@ int phix_stepper_store(phix_stepper_t* h, double* const* fields, void* stream);
 /* Advance nsteps time steps on `stream`.  Each step is one launch per RK
  * stage (4 for RK4, 1 for Euler) with the BCs, the stage combination and the
  * final update fused in; a single-field 2-D RK4 step whose sides are all
- * periodic or zero-flux is one launch for all four stages (see
+ * periodic or zero-flux is one launch for all four stages, and a 3-D RK4 step
+ * of CH or CH+AC with z periodic and x, y periodic or zero-flux is two
+ * launches of two fused stages each, input planes staged by TMA (see
  * phix_stepper_set_fusion).  When steps_per_graph > 0 (see
  * phix_stepper_set_graph) whole groups of steps replay as one CUDA graph.
- * Replaces Solver::advance / VectorSolver::advance (Solver.cu:366-382). */
+ * Replaces Solver::advance / VectorSolver::advance (Solver.cu:366-382;
+ * VectorSolver.cu:186-228). */
 int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream);
+
+/* Reads and clears the stepper's device error flag: PHIX_ERR_TIMEOUT if a
+ * fused 3-D step gave up waiting (2 s) for a plane copy since the last check
+ * (its CTA returned without writing that part of the step), else PHIX_OK.
+ * Synchronous on `stream`.  No reference counterpart. */
+int phix_stepper_status(phix_stepper_t* h, void* stream);
 
 /* Replay groups of `steps_per_graph` steps from a captured CUDA graph
  * (0 disables graphs).  Replaces the driver step loop (Solver::run,
@@ -167,9 +176,16 @@ int phix_stepper_set_graph(phix_stepper_t* h, int steps_per_graph);
  * reference counterpart (the reference runs each term and stage as its own
  * kernels). */
 int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step);
+/* (3-D CH / CH+AC RK4: 1 = the two-launch fused step, 0 = one launch per
+ * stage; same bits.) */
 
-/* Kernel launches one time step takes with the current settings. */
+/* Kernel launches one time step takes with the current settings (per launch
+ * when one launch advances several steps, see phix_stepper_depth). */
 int phix_stepper_launches_per_step(const phix_stepper_t* h);
+/* Temporal-block depth of the current settings: time steps one launch
+ * advances (2 for the temporally blocked pair tiles of phix_stepper_set_tiles,
+ * else 1).  No reference counterpart. */
+int phix_stepper_depth(const phix_stepper_t* h);
 
 /* Tile shape of the 2-D kernels.  One launch per stage: -1 the box tiles
  * (64x16, 256 threads, flat cell loops), 0..3 column-walking tiles (TX x TY =
@@ -178,7 +194,10 @@ int phix_stepper_launches_per_step(const phix_stepper_t* h);
  * 128x32 (512 threads), 128x64 and 256x32 (1024 threads; FP32 only);
  * 6..15 pair tiles (CH with four periodic sides; two cells per thread) of
  * 128x64, 128x32, 128x32, 128x16, 64x32, 64x64, 256x32, 128x28, 64x28, 64x16
- * with 8, 8, 4, 4, 8, 8, 4, 8, 8, 4 row blocks.  Shapes that do not fit in
+ * with 8, 8, 4, 4, 8, 8, 4, 8, 8, 4 row blocks; 16..19 temporally blocked
+ * pair tiles (two RK4 steps per launch on a 16-cell halo, see
+ * phix_stepper_depth) of 64x32, 64x16, 128x16, 64x28 with 8, 4, 4, 8 row
+ * blocks.  Shapes that do not fit in
  * shared memory for the precision are refused when the step runs.
  * PHIX_MULTISTEP steppers with the pair-layout step: 0..5 pair tiles of
  * 128x32, 64x32, 128x16, 64x16, 64x64, 256x16 with 8, 8, 4, 4, 8, 4 row
@@ -233,6 +252,14 @@ int phix_batch_destroy(phix_batch_t* b);
  * Default: 1 wherever it is possible (the faster on B200 in both
  * precisions).  No reference counterpart. */
 int phix_batch_set_fusion(phix_batch_t* b, int one_launch_per_step);
+/* Temporal-block depth of the one-launch step: 2 runs two RK4 steps per
+ * launch (the pair kernels on tiles with a 16-cell halo, the first step's
+ * update kept in shared memory; an odd remaining step runs alone), 1 (the
+ * default) one.  Depth 2 needs the pair kernels, else PHIX_ERR_UNSUPPORTED.
+ * Same bits either way.  phix_batch_depth: the depth in effect.  No
+ * reference counterpart. */
+int phix_batch_set_depth(phix_batch_t* b, int depth);
+int phix_batch_depth(const phix_batch_t* b);
 
 /* Kernel launches one batched time step takes with the current settings. */
 int phix_batch_launches_per_step(const phix_batch_t* b);
@@ -247,8 +274,9 @@ int phix_batch_set_graph(phix_batch_t* b, int steps_per_graph);
 int phix_batch_set_tiles(phix_batch_t* b, int tile_cfg, int ctas_per_sm);
 int phix_batch_get_tiles(const phix_batch_t* b, int* tile_cfg, int* ctas_per_sm, int* ntiles);
 /* Time every tile shape x CTA count of the one-launch-per-stage kernels, and
- * the one-launch step where possible, on trial_steps steps of the real batch
- * (state saved and restored); keep the fastest; *best_ms = ms per step. */
+ * the one-launch step at temporal-block depths 1 and 2 where possible, on
+ * trial_steps steps of the real batch (state saved and restored); keep the
+ * fastest; *best_ms = ms per step. */
 int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms);
 /* FP64 mass (sum of u * dV over physical cells) per instance; synchronous. */
 int phix_batch_mass(phix_batch_t* b, double* masses);
@@ -297,6 +325,13 @@ float* phix_surrogate_grad_ptr(phix_surrogate_t* s);
  * else PHIX_OK.  phix_surrogate_step is asynchronous and does not read the
  * flag; phix_surrogate_grad reads it.  Synchronous on `stream`. */
 int phix_surrogate_status(phix_surrogate_t* s, void* stream);
+/* Measured multiply-add throughput of the current device: *tflops = 2 x
+ * fused multiply-adds per second / 1e12 (best of three launches of a probe
+ * that keeps every SM busy with independent FMA chains).  precision PHIX_F64,
+ * or PHIX_F32 with packed != 0 for the two-lane f32x2 instruction.  The
+ * denominator of the arithmetic-pipe roofline of the stencil kernels.
+ * Synchronous.  No reference counterpart. */
+int phix_measure_fma_peak(int precision, int packed, double* tflops);
 /* Self-test of those bounded waits: one thread waits for an mbarrier of count
  * 1 with a wall-clock limit of limit_s (0 < limit_s <= 2), arriving on it
  * first when `arrive` is non-zero.  Returns PHIX_OK when the wait completed and

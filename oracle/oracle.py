@@ -277,15 +277,15 @@ class Reference:
             raise RuntimeError("ref_lap failed")
 
 
-def build(with_ref: bool | None = None, quiet: bool = True) -> None:
-    """Compile the oracle (and, when the reference tree is present, oracle/_ref)."""
+def build(ref_tree: str | None = None, quiet: bool = True) -> None:
+    """Compile the oracle, and, given the reference project's source tree
+    (`ref_tree`, else $PHIX_REFERENCE_TREE), oracle/_ref and the drop-in
+    driver pairs."""
     import subprocess
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "liboracle.so", "liboracle_omp.so"], check=True, stdout=out)
-    ref_src = os.environ.get("PHIX_REFERENCE_TREE", "/root/reference")
-    if with_ref is None:
-        with_ref = os.path.isdir(os.path.join(ref_src, "src"))
-    if with_ref:
+    ref_src = ref_tree or os.environ.get("PHIX_REFERENCE_TREE")
+    if ref_src and os.path.isdir(os.path.join(ref_src, "src")):
         subprocess.run(["make", "-C", HERE, "-j8", "ref", f"REF={ref_src}"], check=True, stdout=out)
         cxx = os.path.join(os.path.dirname(HERE), "phix_b200", "libphix_cxx.so")
         if os.path.exists(cxx):

@@ -103,9 +103,11 @@ def lib() -> C.CDLL:
         "phix_stepper_load": ([vp, C.POINTER(vp), vp], C.c_int),
         "phix_stepper_store": ([vp, C.POINTER(vp), vp], C.c_int),
         "phix_stepper_advance": ([vp, C.c_int, vp], C.c_int),
+        "phix_stepper_status": ([vp, vp], C.c_int),
         "phix_stepper_set_graph": ([vp, C.c_int], C.c_int),
         "phix_stepper_set_fusion": ([vp, C.c_int], C.c_int),
         "phix_stepper_launches_per_step": ([vp], C.c_int),
+        "phix_stepper_depth": ([vp], C.c_int),
         "phix_stepper_set_tiles": ([vp, C.c_int], C.c_int),
         "phix_stepper_autotune": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
         "phix_stepper_get_tiles": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
@@ -118,6 +120,8 @@ def lib() -> C.CDLL:
         "phix_batch_destroy": ([vp], C.c_int),
         "phix_batch_launches_per_step": ([vp], C.c_int),
         "phix_batch_set_fusion": ([vp, C.c_int], C.c_int),
+        "phix_batch_set_depth": ([vp, C.c_int], C.c_int),
+        "phix_batch_depth": ([vp], C.c_int),
         "phix_batch_load": ([vp, C.c_int, vp, C.c_int, vp], C.c_int),
         "phix_batch_store": ([vp, C.c_int, vp, C.c_int, vp], C.c_int),
         "phix_batch_advance": ([vp, C.c_int, vp], C.c_int),
@@ -140,6 +144,7 @@ def lib() -> C.CDLL:
         "phix_surrogate_grad_ptr": ([vp], C.c_void_p),
         "phix_surrogate_status": ([vp, vp], C.c_int),
         "phix_wait_selftest": ([C.c_int, C.c_double, vp], C.c_int),
+        "phix_measure_fma_peak": ([C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
         "phix_plane_gather": ([vp, vp, C.c_int, C.c_int, C.c_int, vp], C.c_int),
         "phix_plane_scatter": ([vp, vp, C.c_int, C.c_int, C.c_int, vp], C.c_int),
         "phix_stepper_diagnostics": ([vp, P], C.c_int),
@@ -163,6 +168,13 @@ def check(rc: int) -> int:
 
 def launch_count() -> int:
     return int(lib().phix_launch_count())
+
+
+def measure_fma_peak(precision: int, packed: bool = False) -> float:
+    """Measured FMA throughput of the current GPU in TFLOP/s (fma = 2 flops)."""
+    t = C.c_double()
+    check(lib().phix_measure_fma_peak(precision, 1 if packed else 0, C.byref(t)))
+    return t.value
 
 
 def _prm(prm: Sequence[float]):
@@ -271,6 +283,11 @@ class Stepper:
     def advance(self, nsteps: int, stream=None):
         check(lib().phix_stepper_advance(self.h, nsteps, _stream(stream)))
 
+    def status(self, stream=None):
+        """Raise PhixError (ERR_TIMEOUT) if a fused 3-D step gave up waiting
+        for a plane copy since the last check; clears the flag."""
+        check(lib().phix_stepper_status(self.h, _stream(stream)))
+
     def set_graph(self, steps_per_graph: int):
         check(lib().phix_stepper_set_graph(self.h, steps_per_graph))
 
@@ -282,9 +299,15 @@ class Stepper:
     def launches_per_step(self) -> int:
         return lib().phix_stepper_launches_per_step(self.h)
 
+    @property
+    def depth(self) -> int:
+        """Time steps one launch advances (temporal-block depth)."""
+        return lib().phix_stepper_depth(self.h)
+
     def set_tiles(self, cfg: int):
         """2-D tile shape: one launch per stage -1 (box) or 0..3 (column
-        tiles); one launch per RK4 step 0..15 (6..15 pair tiles), -1 by grid."""
+        tiles); one launch per RK4 step 0..19 (6..15 pair tiles, 16..19
+        temporally blocked pair tiles: two steps per launch), -1 by grid."""
         check(lib().phix_stepper_set_tiles(self.h, cfg))
 
     def tiles(self):
@@ -389,6 +412,14 @@ class Batch:
     def set_fusion(self, on: bool):
         """One launch per RK4 step for the whole batch (True) or one per stage."""
         check(lib().phix_batch_set_fusion(self.h, 1 if on else 0))
+
+    def set_depth(self, depth: int):
+        """Temporal-block depth of the one-launch step: 1, or 2 (two RK4 steps per launch)."""
+        check(lib().phix_batch_set_depth(self.h, depth))
+
+    @property
+    def depth(self) -> int:
+        return lib().phix_batch_depth(self.h)
 
     @property
     def launches_per_step(self) -> int:

@@ -85,12 +85,12 @@ template <typename T> struct BatchPair;
 template <> struct BatchPair<float> { static constexpr int TX = 128, TY = 32, NRP = 8; };
 template <> struct BatchPair<double> { static constexpr int TX = 64, TY = 32, NRP = 8; };
 
-template <typename T>
-int batched_pair(bool prepare, const StepArgs<T>* args, const BatchTile* tiles, int ntiles, cudaStream_t s) {
+template <typename T, int NS>
+int batched_pair_ns(bool prepare, const StepArgs<T>* args, const BatchTile* tiles, int ntiles, cudaStream_t s) {
     using C = BatchPair<T>;
-    using G = StepPair<T, C::TX, C::TY, C::NRP>;
+    using G = StepPair<T, C::TX, C::TY, C::NRP, NS>;
     static_assert(G::smem_bytes() <= 227 * 1024, "batched pair tile exceeds shared memory");
-    auto kern = step_pair_batched<T, C::TX, C::TY, C::NRP>;
+    auto kern = step_pair_batched<T, C::TX, C::TY, C::NRP, NS>;
     if (prepare) {
         PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
         return PHIX_OK;
@@ -99,6 +99,18 @@ int batched_pair(bool prepare, const StepArgs<T>* args, const BatchTile* tiles, 
     kern<<<ntiles, G::NT, G::smem_bytes(), s>>>(args, tiles);
     PHIX_LAUNCH_CHECK("step_pair_batched");
     return PHIX_OK;
+}
+
+// depth: time steps per launch (2: the temporally blocked pair kernel)
+template <typename T>
+int batched_pair(bool prepare, const StepArgs<T>* args, const BatchTile* tiles, int ntiles, cudaStream_t s,
+                 int depth = 1) {
+    if (prepare) {
+        int rc = batched_pair_ns<T, 1>(true, args, tiles, ntiles, s);
+        return rc ? rc : batched_pair_ns<T, 2>(true, args, tiles, ntiles, s);
+    }
+    return depth == 2 ? batched_pair_ns<T, 2>(false, args, tiles, ntiles, s)
+                      : batched_pair_ns<T, 1>(false, args, tiles, ntiles, s);
 }
 
 template <typename T, int PHYS, int MODE>
@@ -208,6 +220,9 @@ struct phix_batch {
     // one launch per RK4 step (possible where every side is periodic or zero-flux)
     bool can_fuse = false, fuse_steps = false;
     bool step_pair = false;  // the fused step runs the pair kernels
+    int depth = 1;           // time steps per pair-kernel launch (temporal blocking: 2)
+    int graph_launches[2] = {0, 0};
+    bool graph_flip[2] = {false, false};
     void* step_args_dev = nullptr;  // [parity][ninst] StepArgs
     BatchTile* step_tiles_dev = nullptr;
     int step_ntiles = 0;
@@ -364,12 +379,12 @@ int build_step(phix_batch* b) {
 }
 
 template <typename T>
-int batch_step(phix_batch* b, cudaStream_t s) {
+int batch_step(phix_batch* b, cudaStream_t s, int depth) {
     const int par = b->cur;
     int rc;
     if (b->fuse_steps) {
         const StepArgs<T>* args = reinterpret_cast<const StepArgs<T>*>(b->step_args_dev) + (size_t)par * b->ninst;
-        rc = b->step_pair ? batched_pair<T>(false, args, b->step_tiles_dev, b->step_ntiles, s)
+        rc = b->step_pair ? batched_pair<T>(false, args, b->step_tiles_dev, b->step_ntiles, s, depth)
                           : batched_step<T>(b->phys, false, args, b->step_tiles_dev, b->step_ntiles, b->nsm, s);
         if (rc) return rc;
     } else if (b->scheme == PHIX_EULER) {
@@ -389,10 +404,20 @@ int batch_step(phix_batch* b, cudaStream_t s) {
     return PHIX_OK;
 }
 
-int batch_steps(phix_batch* b, int n, cudaStream_t s) {
-    for (int i = 0; i < n; ++i) {
-        int rc = b->prec == PHIX_F32 ? batch_step<float>(b, s) : batch_step<double>(b, s);
+int batch_depth(const phix_batch* b) { return b->fuse_steps && b->step_pair ? b->depth : 1; }
+
+int batch_launches_per_step(const phix_batch* b) { return b->scheme == PHIX_RK4 && !b->fuse_steps ? 4 : 1; }
+
+// n time steps; with depth 2, pairs of steps per launch and an odd
+// remainder as one single-step launch
+int batch_steps(phix_batch* b, int n, cudaStream_t s, int* launches = nullptr) {
+    const int d = batch_depth(b);
+    for (int i = 0; i < n;) {
+        const int k = d == 2 && n - i >= 2 ? 2 : 1;
+        int rc = b->prec == PHIX_F32 ? batch_step<float>(b, s, k) : batch_step<double>(b, s, k);
         if (rc) return rc;
+        if (launches) *launches += batch_launches_per_step(b);
+        i += k;
     }
     return PHIX_OK;
 }
@@ -402,12 +427,14 @@ int batch_replay(phix_batch* b, cudaStream_t s) {
     if (!b->gexec[parity]) {
         cudaGraph_t graph = nullptr;
         PHIX_TRY_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
-        int rc;
+        int rc, launches = 0;
         {
             LaunchCountPause pause;  // recorded, not launched: the replay below counts them
-            rc = batch_steps(b, b->graph_steps, b->cap);
+            rc = batch_steps(b, b->graph_steps, b->cap, &launches);
         }
         cudaError_t e = cudaStreamEndCapture(b->cap, &graph);
+        b->graph_flip[parity] = b->cur != parity;  // each launch swaps the state buffers
+        b->graph_launches[parity] = launches;
         b->cur = parity;
         if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
         if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
@@ -416,8 +443,8 @@ int batch_replay(phix_batch* b, cudaStream_t s) {
         if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
     }
     PHIX_TRY_CUDA(cudaGraphLaunch(b->gexec[parity], s));
-    count_launch(b->graph_steps * (b->scheme == PHIX_RK4 && !b->fuse_steps ? 4 : 1));
-    if (b->graph_steps % 2) b->cur = 1 - parity;
+    count_launch(b->graph_launches[parity]);
+    if (b->graph_flip[parity]) b->cur = 1 - parity;
     return PHIX_OK;
 }
 
@@ -616,6 +643,21 @@ int phix_batch_set_fusion(phix_batch_t* b, int one_launch_per_step) {
     return PHIX_OK;
 }
 
+int phix_batch_set_depth(phix_batch_t* b, int depth) {
+    if (!b || (depth != 1 && depth != 2)) { set_error("batch_set_depth: bad batch or depth (1 or 2)"); return PHIX_ERR_ARG; }
+    if (depth == 2 && !b->step_pair) {
+        set_error("batch_set_depth: two steps per launch need the pair kernels (CH, four periodic sides)");
+        return PHIX_ERR_UNSUPPORTED;
+    }
+    if (depth != b->depth) {
+        batch_drop_graphs(b);
+        b->depth = depth;
+    }
+    return PHIX_OK;
+}
+
+int phix_batch_depth(const phix_batch_t* b) { return b ? batch_depth(b) : -1; }
+
 int phix_batch_set_graph(phix_batch_t* b, int steps_per_graph) {
     if (!b || steps_per_graph < 0) { set_error("batch_set_graph: bad argument"); return PHIX_ERR_ARG; }
     batch_drop_graphs(b);
@@ -662,7 +704,7 @@ int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms) {
     const int cps_options[] = {0, 2, 4};
     int rc = PHIX_OK;
     auto trial = [&](float* ms) {
-        int r = batch_steps(b, 1, 0);  // warm-up
+        int r = batch_steps(b, batch_depth(b), 0);  // warm-up
         if (r) return r;
         cudaEventRecord(e0, 0);
         if ((r = batch_steps(b, trial_steps, 0))) return r;
@@ -680,13 +722,19 @@ int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms) {
             if (ms < best) { best = ms; best_cfg = cfg; best_cps = cps; }
         }
     }
-    // one launch per RK4 step
+    // one launch per RK4 step, and (pair kernels) two steps per launch
+    int best_depth = b->depth;
     if (!rc && b->can_fuse) {
-        float ms = 0.f;
-        b->fuse_steps = true;
-        rc = trial(&ms);
-        b->fuse_steps = false;
-        if (!rc && ms < best) { best = ms; best_fused = true; }
+        const int depth0 = b->depth;
+        for (int d = 1; d <= (b->step_pair ? 2 : 1) && !rc; ++d) {
+            float ms = 0.f;
+            b->fuse_steps = true;
+            b->depth = d;
+            rc = trial(&ms);
+            b->fuse_steps = false;
+            if (!rc && ms < best) { best = ms; best_fused = true; best_depth = d; }
+        }
+        b->depth = depth0;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -704,6 +752,7 @@ int phix_batch_autotune(phix_batch_t* b, int trial_steps, double* best_ms) {
     if (rc) return rc;
     rc = phix_batch_set_tiles(b, best_cfg, best_cps);
     if (!rc) rc = phix_batch_set_fusion(b, best_fused ? 1 : 0);
+    if (!rc && best_fused) rc = phix_batch_set_depth(b, best_depth);
     if (best_ms) *best_ms = best / trial_steps;
     return rc;
 }

@@ -56,6 +56,26 @@ __global__ void __launch_bounds__(256) f32_pair_to_f64(double* __restrict__ x, c
         x[i] = (double)hi[i] + (double)lo[i];
 }
 
+// The same conversions between a caller array (row pitch sx, S elements) and
+// a stepper array whose rows are padded to pitch pk (>= sx).
+__global__ void __launch_bounds__(256) f64_split_f32_rows(float* __restrict__ hi, float* __restrict__ lo,
+                                                          const double* __restrict__ x, size_t n, int sx, int pk) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / (size_t)sx, d = r * pk + (i - r * sx);
+        const double v = x[i];
+        const float h = (float)v;
+        hi[d] = h;
+        if (lo) lo[d] = (float)(v - (double)h);
+    }
+}
+__global__ void __launch_bounds__(256) f32_rows_to_f64(double* __restrict__ x, const float* __restrict__ hi,
+                                                       const float* __restrict__ lo, size_t n, int sx, int pk) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / (size_t)sx, d = r * pk + (i - r * sx);
+        x[i] = lo ? (double)hi[d] + (double)lo[d] : (double)hi[d];
+    }
+}
+
 static int aligned16(const void* a, const void* b) {
     return ((uintptr_t)a % 16 == 0) && ((uintptr_t)b % 16 == 0);
 }
@@ -98,9 +118,14 @@ int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s
         // that no BC rewrites stay identical whichever buffer is current
         // (the multi-step mu has one buffer)
         const int nb = (stepper_scheme(h) == PHIX_MULTISTEP && f == 1) ? 1 : 2;
+        const int sx = stepper_grid_layout(h).s[1], pk = stepper_layout(h).s[1];
         for (int b = 0; b < nb; ++b) {
             void* dst = stepper_state_buf(h, b, f);
-            if (stepper_prec(h) == PHIX_F64) {
+            if (pk != sx) {  // row-padded FP32 state
+                f64_split_f32_rows<<<conv_grid(S), 256, 0, s>>>((float*)dst, (float*)stepper_lo_buf(h, b, f), fields[f],
+                                                                S, sx, pk);
+                PHIX_LAUNCH_CHECK("f64_split_f32_rows");
+            } else if (stepper_prec(h) == PHIX_F64) {
                 if (dst == (const void*)fields[f]) continue;
                 PHIX_TRY_CUDA(cudaMemcpyAsync(dst, fields[f], S * sizeof(double), cudaMemcpyDeviceToDevice, s));
             } else if (stepper_lo_buf(h, b, f)) {
@@ -121,7 +146,13 @@ int stepper_copy_out(phix_stepper* h, double* const* fields, cudaStream_t s) {
     for (int f = 0; f < stepper_nf(h); ++f) {
         if (!fields[f]) { set_error("store: field %d is NULL", f); return PHIX_ERR_ARG; }
         const void* src = stepper_state(h, f);
-        if (stepper_prec(h) == PHIX_F64) {
+        const int sx = stepper_grid_layout(h).s[1], pk = stepper_layout(h).s[1];
+        if (pk != sx) {  // row-padded FP32 state
+            const bool multi_mu = stepper_scheme(h) == PHIX_MULTISTEP && f == 1;
+            const void* lo = multi_mu ? nullptr : stepper_lo_buf(h, stepper_cur(h), f);
+            f32_rows_to_f64<<<conv_grid(S), 256, 0, s>>>(fields[f], (const float*)src, (const float*)lo, S, sx, pk);
+            PHIX_LAUNCH_CHECK("f32_rows_to_f64");
+        } else if (stepper_prec(h) == PHIX_F64) {
             if (src == (const void*)fields[f]) continue;
             PHIX_TRY_CUDA(cudaMemcpyAsync(fields[f], src, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
         } else {

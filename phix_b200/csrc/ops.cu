@@ -131,6 +131,14 @@ int bc_fill(T* field, const phix_grid_t* g, bool low_part, cudaStream_t s) {
     Layout L;
     int rc = validate_grid(g, &L, nullptr);
     if (rc) return rc;
+    return bc_fill_layout<T>(field, g, L, low_part, s);
+}
+
+// The same on an array of layout L (the grid's, or a stepper's row-padded
+// internal copy: the padding columns past the x ghosts are never read).
+template <typename T>
+int bc_fill_layout(T* field, const phix_grid_t* g, const Layout& L, bool low_part, cudaStream_t s) {
+    int rc;
     auto launch = [&](int axis, int type, int lo, int hi) -> int {
         const int sx = L.s[1], sy = L.s[2] / L.s[1], sz = L.n[2] + 2 * L.ghost;
         long long faces = axis == 0 ? (long long)sy * sz : axis == 1 ? (long long)sx * sz : (long long)sx * sy;
@@ -156,6 +164,8 @@ int bc_fill(T* field, const phix_grid_t* g, bool low_part, cudaStream_t s) {
 }
 template int bc_fill<float>(float*, const phix_grid_t*, bool, cudaStream_t);
 template int bc_fill<double>(double*, const phix_grid_t*, bool, cudaStream_t);
+template int bc_fill_layout<float>(float*, const phix_grid_t*, const Layout&, bool, cudaStream_t);
+template int bc_fill_layout<double>(double*, const phix_grid_t*, const Layout&, bool, cudaStream_t);
 
 }  // namespace phix
 

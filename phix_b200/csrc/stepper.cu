@@ -23,7 +23,10 @@
 #include "phix/detail/step2d.cuh"
 #include "phix/detail/step2d_pair.cuh"
 #include "phix/detail/step2d_pair_ms.cuh"
+#include "phix/detail/march3d_fused.cuh"
 #include "stepper.h"
+
+#include <cudaTypedefs.h>
 
 namespace phix {
 
@@ -165,10 +168,13 @@ constexpr int kStepCfgs[][3] = {{64, 16, 256}, {64, 32, 256}, {128, 16, 256}, {1
                                  {256, 32, 1024}};
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100
 constexpr int kNumStepCfgs = sizeof(kStepCfgs) / sizeof(kStepCfgs[0]);
-// tiles of the pair kernels (CH, four periodic sides): (TX, TY, row blocks);
-// threads = (TX / 2 + 8) x row blocks.  Step configuration kNumStepCfgs + i.
-constexpr int kPairCfgs[][3] = {{128, 64, 8}, {128, 32, 8}, {128, 32, 4}, {128, 16, 4}, {64, 32, 8},
-                                 {64, 64, 8},  {256, 32, 4}, {128, 28, 8}, {64, 28, 8},  {64, 16, 4}};
+// tiles of the pair kernels (CH, four periodic sides): (TX, TY, row blocks,
+// time steps per launch); threads = (TX / 2 + 8 depth) x row blocks.  Step
+// configuration kNumStepCfgs + i.  The last four are temporally blocked:
+// two RK4 steps per launch on a tile with a 16-cell halo.
+constexpr int kPairCfgs[][4] = {{128, 64, 8, 1}, {128, 32, 8, 1}, {128, 32, 4, 1}, {128, 16, 4, 1}, {64, 32, 8, 1},
+                                 {64, 64, 8, 1},  {256, 32, 4, 1}, {128, 28, 8, 1}, {64, 28, 8, 1},  {64, 16, 4, 1},
+                                 {64, 32, 8, 2},  {64, 16, 4, 2},  {128, 16, 4, 2}, {64, 28, 8, 2}};
 constexpr int kNumPairCfgs = sizeof(kPairCfgs) / sizeof(kPairCfgs[0]);
 
 template <typename T, class Pol, int TX, int TY, int NT>
@@ -210,9 +216,9 @@ int step_dispatch(int cfg, bool prepare, const StepArgs<T>* A, cudaStream_t s) {
 
 // prepare: set the shared-memory attribute; occ != nullptr: report resident
 // CTAs per SM (0: does not fit); else launch.
-template <typename T, int TX, int TY, int NRP>
+template <typename T, int TX, int TY, int NRP, int NS>
 int pair_cfg(bool prepare, const StepArgs<T>* A, cudaStream_t s, int* occ = nullptr) {
-    using G = StepPair<T, TX, TY, NRP>;
+    using G = StepPair<T, TX, TY, NRP, NS>;
     if (G::smem_bytes() > kMaxSmem) {
         if (occ) *occ = 0;
         if (prepare || occ) return PHIX_OK;
@@ -220,17 +226,17 @@ int pair_cfg(bool prepare, const StepArgs<T>* A, cudaStream_t s, int* occ = null
         return PHIX_ERR_UNSUPPORTED;
     }
     if (occ) {
-        PHIX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, step_pair<T, TX, TY, NRP>, G::NT,
+        PHIX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, step_pair<T, PolCH, TX, TY, NRP, NS>, G::NT,
                                                                     G::smem_bytes()));
         return PHIX_OK;
     }
     if (prepare) {
-        PHIX_TRY_CUDA(cudaFuncSetAttribute(step_pair<T, TX, TY, NRP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        PHIX_TRY_CUDA(cudaFuncSetAttribute(step_pair<T, PolCH, TX, TY, NRP, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)G::smem_bytes()));
         return PHIX_OK;
     }
     dim3 grid((A->S.L.n[0] + TX - 1) / TX, (A->S.L.n[1] + TY - 1) / TY, 1);
-    step_pair<T, TX, TY, NRP><<<grid, G::NT, G::smem_bytes(), s>>>(*A);
+    step_pair<T, PolCH, TX, TY, NRP, NS><<<grid, G::NT, G::smem_bytes(), s>>>(*A, PolCH{});
     PHIX_LAUNCH_CHECK("step_pair");
     return PHIX_OK;
 }
@@ -239,7 +245,7 @@ template <typename T>
 int pair_dispatch(int i, bool prepare, const StepArgs<T>* A, cudaStream_t s, int* occ = nullptr) {
     switch (i) {
 #define PHIX_PAIR_CASE(i) \
-    case i: return pair_cfg<T, kPairCfgs[i][0], kPairCfgs[i][1], kPairCfgs[i][2]>(prepare, A, s, occ);
+    case i: return pair_cfg<T, kPairCfgs[i][0], kPairCfgs[i][1], kPairCfgs[i][2], kPairCfgs[i][3]>(prepare, A, s, occ);
         PHIX_PAIR_CASE(0)
         PHIX_PAIR_CASE(1)
         PHIX_PAIR_CASE(2)
@@ -250,6 +256,10 @@ int pair_dispatch(int i, bool prepare, const StepArgs<T>* A, cudaStream_t s, int
         PHIX_PAIR_CASE(7)
         PHIX_PAIR_CASE(8)
         PHIX_PAIR_CASE(9)
+        PHIX_PAIR_CASE(10)
+        PHIX_PAIR_CASE(11)
+        PHIX_PAIR_CASE(12)
+        PHIX_PAIR_CASE(13)
 #undef PHIX_PAIR_CASE
     }
     set_error("step_pair: bad tile configuration %d", i);
@@ -369,6 +379,7 @@ int pick_pair_cfg(const Layout& L, int nsm) {
     int best = 1;
     double best_cost = 1e300;
     for (int i = 0; i < kNumPairCfgs; ++i) {
+        if (kPairCfgs[i][3] != 1) continue;  // the default is one step per launch
         int occ = 0;
         if (pair_dispatch<T>(i, false, nullptr, 0, &occ) != PHIX_OK || occ < 2) continue;
         const int tx = kPairCfgs[i][0], ty = kPairCfgs[i][1];
@@ -415,9 +426,24 @@ int launch_ms(const StageArgs<T>& A, cudaStream_t s, int tile) {
     return ms_dispatch<T>(cfg, false, &A, s);
 }
 
+// Time steps one launch of step configuration `tile` advances (1, or 2 for
+// the temporally blocked pair tiles).
+int step_cfg_depth(int tile) {
+    return tile >= kNumStepCfgs && tile < kNumStepCfgs + kNumPairCfgs ? kPairCfgs[tile - kNumStepCfgs][3] : 1;
+}
+
+// One launch advancing `depth` steps (a depth-1 launch of a depth-2
+// configuration takes the grid's default single-step shape).
 template <typename T>
-int launch_step2d(int phys, const StepArgs<T>& A, cudaStream_t s, int tile) {
-    const int cfg = tile < 0 ? default_step_cfg<T>(phys, A.S.L) : tile;
+int launch_step2d(int phys, const StepArgs<T>& A, cudaStream_t s, int tile, int depth = 1) {
+    int cfg = tile < 0 ? default_step_cfg<T>(phys, A.S.L) : tile;
+    if (step_cfg_depth(cfg) != depth) {
+        if (depth != 1) {
+            set_error("step_pair: configuration %d does not take %d steps per launch", cfg, depth);
+            return PHIX_ERR_ARG;
+        }
+        cfg = default_step_cfg<T>(phys, A.S.L);
+    }
     if (cfg >= kNumStepCfgs) {
         if (phys != PHIX_PHYS_CH || !step_pair_supported(A.S.L, 2)) {
             set_error("step_pair: tile configuration %d needs CH with four periodic sides", cfg);
@@ -526,8 +552,10 @@ struct phix_stepper {
     double prm[8] = {0};
     double dt = 0.0;
     phix_grid_t g{};
-    Layout L{};
-    size_t S = 0;      // stored elements per field
+    Layout L{};        // the grid's stored layout (callers' arrays)
+    Layout Lk{};       // layout of the stepper's own arrays (rows padded for 3-D FP32)
+    size_t S = 0;      // stored elements per field (callers' arrays)
+    size_t Sk = 0;     // elements per field of the stepper's own arrays
     size_t esz = 8;    // element size of the state
     void* st[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     void* lo[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // FP32: low parts of the state
@@ -545,12 +573,153 @@ struct phix_stepper {
     cudaStream_t cap = nullptr;
     int graph_steps = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int graph_launches[2] = {0, 0};       // kernel launches recorded in each graph
+    bool graph_flip[2] = {false, false};  // whether replaying it swaps the state buffers
+    int* err = nullptr;            // device flag: a fused 3-D step gave up waiting for a plane copy
+    bool fuse3d = true;            // 3-D RK4 of the mu physics: two launches of two fused stages
     double* stage_host = nullptr;  // device FP64 staging for run_host / diagnostics
     double* partials = nullptr;
     int partials_n = 0;
 };
 
 namespace phix {
+
+// ---------------------------------------------------------------------------
+// 3-D RK4 of the mu physics: two launches of two fused stages
+// (march3d_fused.cuh), input planes by TMA
+// ---------------------------------------------------------------------------
+namespace {
+
+// tiles (TX, TY, threads) of launch A (stages 1-2) and launch B (stages 3-4):
+// the largest that keep two CTAs per SM for FP32 A (113 KB of shared memory)
+// and fit one CTA per SM otherwise
+template <typename T> struct M2Cfg;
+template <> struct M2Cfg<float> {
+    static constexpr int AX = 32, AY = 16, ANT = 256, BX = 32, BY = 16, BNT = 512;
+};
+template <> struct M2Cfg<double> {
+    static constexpr int AX = 32, AY = 16, ANT = 512, BX = 32, BY = 8, BNT = 512;
+};
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// Tensor map over a stored array of layout L (x, y, z = row, rows, planes;
+// the padding columns of a row-padded layout are in bounds), boxes of
+// WB x HB x 1 elements, no swizzle, zero fill outside.
+int plane_map(CUtensorMap* m, const void* base, const Layout& L, int esz, int WB, int HB) {
+    auto enc = tensor_map_encoder();
+    if (!enc) { set_error("cuTensorMapEncodeTiled is not available"); return PHIX_ERR_UNSUPPORTED; }
+    const int sy = L.s[2] / L.s[1], sz = L.n[2] + 2 * L.ghost;
+    cuuint64_t dims[3] = {(cuuint64_t)L.s[1], (cuuint64_t)sy, (cuuint64_t)sz};
+    cuuint64_t strides[2] = {(cuuint64_t)L.s[1] * esz, (cuuint64_t)L.s[2] * esz};
+    cuuint32_t box[3] = {(cuuint32_t)WB, (cuuint32_t)HB, 1u};
+    cuuint32_t estr[3] = {1u, 1u, 1u};
+    const CUresult r = enc(m, esz == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                           const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled failed (%d)", (int)r); return PHIX_ERR_CUDA; }
+    return PHIX_OK;
+}
+
+// Output planes per CTA: the z chunking of the tile columns that takes the
+// fewest (waves x planes marched per CTA), a CTA marching rz + 2E planes.
+int pick_rz(long long columns, int n2, int slots, int E) {
+    int best_rz = n2;
+    double best = 1e300;
+    for (int nzc = 1; nzc <= (n2 + 7) / 8; ++nzc) {
+        const int rz = (n2 + nzc - 1) / nzc;
+        const long long ctas = columns * ((n2 + rz - 1) / rz);
+        const long long waves = (ctas + slots - 1) / slots;
+        const double cost = (double)waves * (rz + 2 * E);
+        if (cost < best) { best = cost; best_rz = rz; }
+    }
+    return best_rz;
+}
+
+template <typename T, class Pol, int TX, int TY, int NT, bool B>
+int m2_kernel(bool prepare, March2Args<T>* a, cudaStream_t s) {
+    using G = March2<T, Pol, TX, TY, B>;
+    static_assert(G::smem_bytes() <= 227 * 1024, "fused 3-D tile too large");
+    auto kern = stage2_march3d<T, Pol, TX, TY, NT, B>;
+    if (prepare) {
+        PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
+        return PHIX_OK;
+    }
+    static int slots = 0;  // resident CTAs on the device
+    if (!slots) {
+        int dev = 0, nsm = 0, occ = 0;
+        PHIX_TRY_CUDA(cudaGetDevice(&dev));
+        PHIX_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        PHIX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, G::smem_bytes()));
+        slots = (occ > 0 ? occ : 1) * nsm;
+    }
+    const Layout& L = a->S.L;
+    int rc;
+    for (int f = 0; f < G::NF; ++f) {
+        if ((rc = plane_map(&a->tu[f], a->S.u[f], L, (int)sizeof(T), G::WB, G::HB))) return rc;
+        if (B && (rc = plane_map(&a->tk[f], a->k2[f], L, (int)sizeof(T), G::WB, G::HB))) return rc;
+    }
+    const long long cols = (long long)((L.n[0] + TX - 1) / TX) * ((L.n[1] + TY - 1) / TY);
+    a->rz = pick_rz(cols, L.n[2], slots, G::E);
+    dim3 grid((L.n[0] + TX - 1) / TX, (L.n[1] + TY - 1) / TY, (L.n[2] + a->rz - 1) / a->rz);
+    kern<<<grid, NT, G::smem_bytes(), s>>>(*a);
+    PHIX_LAUNCH_CHECK(B ? "stage2_march3d(B)" : "stage2_march3d(A)");
+    return PHIX_OK;
+}
+
+template <typename T, class Pol>
+int m2_step(bool prepare, March2Args<T>* a, cudaStream_t s, bool second) {
+    using C = M2Cfg<T>;
+    if (prepare) {
+        int rc = m2_kernel<T, Pol, C::AX, C::AY, C::ANT, false>(true, nullptr, s);
+        return rc ? rc : m2_kernel<T, Pol, C::BX, C::BY, C::BNT, true>(true, nullptr, s);
+    }
+    return second ? m2_kernel<T, Pol, C::BX, C::BY, C::BNT, true>(false, a, s)
+                  : m2_kernel<T, Pol, C::AX, C::AY, C::ANT, false>(false, a, s);
+}
+
+template <typename T>
+int m2_dispatch(int phys, bool prepare, March2Args<T>* a, cudaStream_t s, bool second) {
+    if (phys == PHIX_PHYS_CH) return m2_step<T, PolCH>(prepare, a, s, second);
+    if (phys == PHIX_PHYS_CHAC) return m2_step<T, PolCHAC>(prepare, a, s, second);
+    set_error("fused 3-D step: physics %d has no chemical potential", phys);
+    return PHIX_ERR_UNSUPPORTED;
+}
+
+}  // namespace
+
+// The fused 3-D path takes the grid: RK4 of CH or CH+AC, z periodic, x and y
+// periodic or zero-flux, rows of whole 16-byte units, 16-byte aligned arrays.
+static bool step3d_fused(const phix_stepper* h) {
+    if (!h->fuse_steps || !h->fuse3d || h->scheme != PHIX_RK4 || h->dim != 3) return false;
+    if (h->phys != PHIX_PHYS_CH && h->phys != PHIX_PHYS_CHAC) return false;
+    const Layout& L = h->Lk;
+    for (int i = 0; i < 4; ++i)
+        if (L.bc[i] != PHIX_BC_PERIODIC && L.bc[i] != PHIX_BC_NOFLUX) return false;
+    if (L.bc[4] != PHIX_BC_PERIODIC) return false;
+    if ((L.s[1] * h->esz) % 16 != 0) return false;
+    const int nfb = h->nf;
+    for (int f = 0; f < nfb; ++f)
+        for (int b = 0; b < 2; ++b)
+            if ((uintptr_t)h->st[b][f] % 16 != 0) return false;
+    return tensor_map_encoder() != nullptr;
+}
 
 static void drop_graphs(phix_stepper* h) {
     for (auto& e : h->gexec)
@@ -568,14 +737,15 @@ static bool ms_pair(const phix_stepper* h) {
 }
 
 static int launches_per_step(const phix_stepper* h) {
+    if (step3d_fused(h)) return 2;
     return h->scheme == PHIX_RK4 && !step_fused(h) ? 4 : 1;
 }
 
 template <typename T>
-static int enqueue_step(phix_stepper* h, cudaStream_t s) {
+static int enqueue_step(phix_stepper* h, cudaStream_t s, int depth) {
     StageArgs<T> A;
     memset(&A, 0, sizeof(A));
-    A.L = h->L;
+    A.L = h->Lk;
     for (int a = 0; a < 3; ++a) A.i2[a] = a < h->dim ? (T)(1.0 / (h->g.d[a] * h->g.d[a])) : (T)0;
     make_coeffs<T>(h->phys, h->prm, A.p);
     const int c = h->cur, o = 1 - c;
@@ -611,7 +781,26 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
         B.S = A;
         B.dt2 = (T)(h->dt * 0.5);
         B.dt = (T)h->dt;
-        if ((rc = launch_step2d<T>(h->phys, B, s, h->tile))) return rc;
+        if ((rc = launch_step2d<T>(h->phys, B, s, h->tile, depth))) return rc;
+    } else if (step3d_fused(h)) {
+        // launch A: k2 and acc = k1 + 2 k2; launch B: the new state
+        const T dt2 = (T)(h->dt * 0.5), dtt = (T)h->dt;
+        for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->st[o][f];
+        A.dtf = (T)(h->dt / 6.0);
+        set_lo(h->nf);
+        March2Args<T> M;
+        memset(&M, 0, sizeof(M));
+        M.S = A;
+        for (int f = 0; f < h->nf; ++f) {
+            M.k2[f] = (T*)h->kbuf[1][f];
+            M.acc[f] = (T*)h->kbuf[0][f];
+        }
+        M.err = h->err;
+        M.a_in = dt2;
+        M.a_mid = dt2;
+        if ((rc = m2_dispatch<T>(h->phys, false, &M, s, false))) return rc;
+        M.a_mid = dtt;
+        if ((rc = m2_dispatch<T>(h->phys, false, &M, s, true))) return rc;
     } else {
         const T dt2 = (T)(h->dt * 0.5), dtt = (T)h->dt;
         // stage 1
@@ -642,10 +831,18 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s) {
     return PHIX_OK;
 }
 
-static int enqueue_steps(phix_stepper* h, int n, cudaStream_t s) {
-    for (int i = 0; i < n; ++i) {
-        int rc = h->prec == PHIX_F32 ? enqueue_step<float>(h, s) : enqueue_step<double>(h, s);
+// Time steps per launch of the current settings: 2 for a temporally blocked
+// pair tile (an odd remainder of steps runs as one single-step launch).
+static int step_depth(const phix_stepper* h) { return step_fused(h) ? step_cfg_depth(h->tile) : 1; }
+
+static int enqueue_steps(phix_stepper* h, int n, cudaStream_t s, int* launches = nullptr) {
+    const int d = step_depth(h);
+    for (int i = 0; i < n;) {
+        const int k = d == 2 && n - i >= 2 ? 2 : 1;
+        int rc = h->prec == PHIX_F32 ? enqueue_step<float>(h, s, k) : enqueue_step<double>(h, s, k);
         if (rc) return rc;
+        if (launches) *launches += launches_per_step(h);
+        i += k;
     }
     return PHIX_OK;
 }
@@ -655,12 +852,14 @@ static int replay_group(phix_stepper* h, cudaStream_t s) {
     if (!h->gexec[parity]) {
         cudaGraph_t graph = nullptr;
         PHIX_TRY_CUDA(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
-        int rc;
+        int rc, launches = 0;
         {
             LaunchCountPause pause;  // recorded, not launched: the replay below counts them
-            rc = enqueue_steps(h, h->graph_steps, h->cap);
+            rc = enqueue_steps(h, h->graph_steps, h->cap, &launches);
         }
         cudaError_t e = cudaStreamEndCapture(h->cap, &graph);
+        h->graph_flip[parity] = h->cur != parity;  // each launch swaps the state buffers
+        h->graph_launches[parity] = launches;
         if (rc) { if (graph) cudaGraphDestroy(graph); h->cur = parity; return rc; }
         if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
         e = cudaGraphInstantiate(&h->gexec[parity], graph, 0);
@@ -670,8 +869,8 @@ static int replay_group(phix_stepper* h, cudaStream_t s) {
     }
     PHIX_TRY_CUDA(cudaGraphLaunch(h->gexec[parity], s));
     // launches inside the graph count as kernel launches of this library
-    count_launch(h->graph_steps * launches_per_step(h));
-    if (h->graph_steps % 2) h->cur = 1 - parity;
+    count_launch(h->graph_launches[parity]);
+    if (h->graph_flip[parity]) h->cur = 1 - parity;
     return PHIX_OK;
 }
 
@@ -711,10 +910,23 @@ int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precisio
     h->L = L;
     h->S = S;
     h->esz = precision == PHIX_F32 ? 4 : 8;
+    // 3-D FP32 steppers keep their arrays with rows padded to whole 16-byte
+    // units (a TMA row stride must be one); the ghost layers stay where the
+    // layout's origin puts them, the padding columns are never read
+    h->Lk = L;
+    h->Sk = S;
+    if (precision == PHIX_F32 && g->dim == 3) {
+        const int sx = L.s[1], pk = (sx + 3) / 4 * 4, sy = L.s[2] / L.s[1], gh = L.ghost;
+        h->Lk.s[1] = pk;
+        h->Lk.s[2] = pk * sy;
+        h->Lk.origin = gh + pk * (gh + sy * gh);
+        h->Sk = (size_t)pk * sy * (L.n[2] + 2 * gh);
+    }
     // measured on B200 at 1024^2: the one-launch step wins in FP32, and in FP64
     // where the pair kernel takes the grid (CH, four periodic sides); the
     // cell-per-thread step kernel loses to one launch per stage in FP64
-    h->fuse_steps = precision == PHIX_F32 || (phys == PHIX_PHYS_CH && step_pair_supported(L, g->dim));
+    h->fuse_steps = precision == PHIX_F32 || (phys == PHIX_PHYS_CH && step_pair_supported(L, g->dim)) ||
+                    (g->dim == 3 && phys != PHIX_PHYS_AC);
     auto fail = [&](cudaError_t e, const char* w) {
         int r = cuda_status(e, w);
         phix_stepper_destroy(h);
@@ -723,29 +935,39 @@ int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precisio
     cudaError_t e;
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < h->nf; ++f) {
-            if ((e = cudaMalloc(&h->st[b][f], S * h->esz)) != cudaSuccess) return fail(e, "cudaMalloc(state)");
-            if ((e = cudaMemset(h->st[b][f], 0, S * h->esz)) != cudaSuccess) return fail(e, "cudaMemset(state)");
+            if ((e = cudaMalloc(&h->st[b][f], h->Sk * h->esz)) != cudaSuccess) return fail(e, "cudaMalloc(state)");
+            if ((e = cudaMemset(h->st[b][f], 0, h->Sk * h->esz)) != cudaSuccess) return fail(e, "cudaMemset(state)");
         }
     if (precision == PHIX_F32) {
         // the multi-step mu is recomputed every step: no low part
         const int nlo = scheme == PHIX_MULTISTEP ? 1 : h->nf;
         for (int b = 0; b < 2; ++b)
             for (int f = 0; f < nlo; ++f) {
-                if ((e = cudaMalloc(&h->lo[b][f], S * 4)) != cudaSuccess) return fail(e, "cudaMalloc(lo)");
-                if ((e = cudaMemset(h->lo[b][f], 0, S * 4)) != cudaSuccess) return fail(e, "cudaMemset(lo)");
+                if ((e = cudaMalloc(&h->lo[b][f], h->Sk * 4)) != cudaSuccess) return fail(e, "cudaMalloc(lo)");
+                if ((e = cudaMemset(h->lo[b][f], 0, h->Sk * 4)) != cudaSuccess) return fail(e, "cudaMemset(lo)");
             }
     }
     if (scheme == PHIX_RK4)
         for (int k = 0; k < 3; ++k)
             for (int f = 0; f < h->nf; ++f) {
                 // ghosts of k stay zero: kernels only ever write physical cells
-                if ((e = cudaMalloc(&h->kbuf[k][f], S * h->esz)) != cudaSuccess) return fail(e, "cudaMalloc(k)");
-                if ((e = cudaMemset(h->kbuf[k][f], 0, S * h->esz)) != cudaSuccess) return fail(e, "cudaMemset(k)");
+                if ((e = cudaMalloc(&h->kbuf[k][f], h->Sk * h->esz)) != cudaSuccess) return fail(e, "cudaMalloc(k)");
+                if ((e = cudaMemset(h->kbuf[k][f], 0, h->Sk * h->esz)) != cudaSuccess) return fail(e, "cudaMemset(k)");
             }
+    if ((e = cudaMalloc(&h->err, sizeof(int))) != cudaSuccess) return fail(e, "cudaMalloc(err)");
+    if ((e = cudaMemset(h->err, 0, sizeof(int))) != cudaSuccess) return fail(e, "cudaMemset(err)");
     if ((e = cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "cudaStreamCreate");
     if ((rc = prepare_stage(phys, g->dim, precision))) {
         phix_stepper_destroy(h);
         return rc;
+    }
+    if (g->dim == 3 && scheme == PHIX_RK4 && phys != PHIX_PHYS_AC) {
+        rc = precision == PHIX_F32 ? m2_dispatch<float>(phys, true, nullptr, 0, false)
+                                   : m2_dispatch<double>(phys, true, nullptr, 0, false);
+        if (rc) {
+            phix_stepper_destroy(h);
+            return rc;
+        }
     }
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e, "cudaDeviceSynchronize");
     *out = h;
@@ -767,6 +989,7 @@ int phix_stepper_destroy(phix_stepper_t* h) {
             if (p) cudaFree(p);
     if (h->stage_host) cudaFree(h->stage_host);
     if (h->partials) cudaFree(h->partials);
+    if (h->err) cudaFree(h->err);
     if (h->cap) cudaStreamDestroy(h->cap);
     delete h;
     return PHIX_OK;
@@ -794,6 +1017,8 @@ int phix_stepper_set_fusion(phix_stepper_t* h, int one_launch_per_step) {
 }
 
 int phix_stepper_launches_per_step(const phix_stepper_t* h) { return h ? launches_per_step(h) : -1; }
+
+int phix_stepper_depth(const phix_stepper_t* h) { return h ? step_depth(h) : -1; }
 
 int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg) {
     if (!h || tile_cfg < -1 || tile_cfg >= (kNumColCfgs > kNumStepCfgs + kNumPairCfgs ? kNumColCfgs
@@ -831,6 +1056,7 @@ int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms) {
             for (int t = -1; t < kNumColCfgs; ++t) cand.push_back({false, t});
         else
             cand.push_back({false, -1});
+        if (h->dim == 3 && h->scheme == PHIX_RK4 && h->phys != PHIX_PHYS_AC) cand.push_back({true, -1});
         if (h->scheme == PHIX_RK4 && h->nf == 1 && step2d_supported(h->L, h->dim))
             for (int t = 0; t < kNumStepCfgs + kNumPairCfgs; ++t) cand.push_back({true, t});
     }
@@ -839,7 +1065,7 @@ int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms) {
     const int cur0 = h->cur;
     const bool bc0 = h->bc_pending, fuse0 = h->fuse_steps;
     const int tile0 = h->tile, graph0 = h->graph_steps;
-    const size_t bytes = h->S * h->esz;
+    const size_t bytes = h->Sk * h->esz;
     const int parts = h->lo[cur0][0] ? 2 : 1;
     void* save = nullptr;
     PHIX_TRY_CUDA(cudaMalloc(&save, bytes * h->nf * parts));
@@ -869,7 +1095,7 @@ int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms) {
     for (size_t c = 0; c < cand.size() && !rc; ++c) {
         h->fuse_steps = cand[c].first;
         h->tile = cand[c].second;
-        int r = enqueue_steps(h, 1, 0);  // warm-up; shapes this grid cannot take are skipped
+        int r = enqueue_steps(h, step_depth(h), 0);  // warm-up; shapes this grid cannot take are skipped
         if (r == PHIX_ERR_UNSUPPORTED) continue;
         if (r) { rc = r; break; }
         float ms = 1e30f;
@@ -927,6 +1153,17 @@ int phix_stepper_bind(phix_stepper_t* h, double* const* fields, double* const* a
     return PHIX_OK;
 }
 
+int phix_stepper_status(phix_stepper_t* h, void* stream) {
+    if (!h) { set_error("status: NULL stepper"); return PHIX_ERR_ARG; }
+    cudaStream_t s = (cudaStream_t)stream;
+    int herr = 0;
+    PHIX_TRY_CUDA(cudaMemcpyAsync(&herr, h->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PHIX_TRY_CUDA(cudaMemsetAsync(h->err, 0, sizeof(int), s));
+    PHIX_TRY_CUDA(cudaStreamSynchronize(s));
+    if (herr) { set_error("stepper: a fused 3-D step gave up waiting for a plane copy"); return PHIX_ERR_TIMEOUT; }
+    return PHIX_OK;
+}
+
 int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream) {
     if (!h || nsteps < 0) { set_error("advance: bad stepper or nsteps"); return PHIX_ERR_ARG; }
     if (!h->st[0][0]) { set_error("advance: stepper has no state buffers"); return PHIX_ERR_ARG; }
@@ -939,10 +1176,10 @@ int phix_stepper_advance(phix_stepper_t* h, int nsteps, void* stream) {
     if (h->bc_pending && nsteps > 0) {
         for (int f = 0; f < h->nf; ++f)
             for (int b = 0; b < (h->scheme == PHIX_MULTISTEP && f == 1 ? 1 : 2); ++b) {  // one mu buffer
-                if (h->prec == PHIX_F64) rc = bc_fill<double>((double*)h->st[b][f], &h->g, false, s);
-                else rc = bc_fill<float>((float*)h->st[b][f], &h->g, false, s);
+                if (h->prec == PHIX_F64) rc = bc_fill_layout<double>((double*)h->st[b][f], &h->g, h->Lk, false, s);
+                else rc = bc_fill_layout<float>((float*)h->st[b][f], &h->g, h->Lk, false, s);
                 if (rc) return rc;
-                if (h->lo[b][f] && (rc = bc_fill<float>((float*)h->lo[b][f], &h->g, true, s))) return rc;
+                if (h->lo[b][f] && (rc = bc_fill_layout<float>((float*)h->lo[b][f], &h->g, h->Lk, true, s))) return rc;
             }
         h->bc_pending = false;
     }
@@ -975,6 +1212,8 @@ void* stepper_state_buf(phix_stepper* h, int b, int f) { return h->st[b][f]; }
 void* stepper_lo_buf(phix_stepper* h, int b, int f) { return h->lo[b][f]; }
 int stepper_cur(const phix_stepper* h) { return h->cur; }
 size_t stepper_stored(const phix_stepper* h) { return h->S; }
+const Layout& stepper_layout(const phix_stepper* h) { return h->Lk; }
+const Layout& stepper_grid_layout(const phix_stepper* h) { return h->L; }
 int stepper_prec(const phix_stepper* h) { return h->prec; }
 int stepper_nf(const phix_stepper* h) { return h->nf; }
 int stepper_phys(const phix_stepper* h) { return h->phys; }

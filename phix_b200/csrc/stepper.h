@@ -23,6 +23,10 @@ void* stepper_state_buf(phix_stepper* h, int b, int f);
 void* stepper_lo_buf(phix_stepper* h, int b, int f);
 int stepper_cur(const phix_stepper* h);
 size_t stepper_stored(const phix_stepper* h);
+// Layout of the stepper's own arrays: the grid's, except that 3-D FP32
+// steppers pad each stored row to a multiple of 16 bytes (TMA row strides).
+const Layout& stepper_layout(const phix_stepper* h);
+const Layout& stepper_grid_layout(const phix_stepper* h);
 int stepper_prec(const phix_stepper* h);
 int stepper_nf(const phix_stepper* h);
 int stepper_phys(const phix_stepper* h);
@@ -36,6 +40,7 @@ double* stepper_partials(phix_stepper* h, int n);
 // All BCs of g applied to a stored array (ops.cu); low_part: the array is the
 // low part of a compensated state.
 template <typename T> int bc_fill(T* field, const phix_grid_t* g, bool low_part, cudaStream_t s);
+template <typename T> int bc_fill_layout(T* field, const phix_grid_t* g, const Layout& L, bool low_part, cudaStream_t s);
 
 // FP64 <-> FP32 copies of n stored elements (convert.cu)
 int convert_f64_to_f32(float* dst, const double* src, size_t n, cudaStream_t s);

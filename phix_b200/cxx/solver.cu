@@ -617,6 +617,15 @@ void Solver::fusedAdvance() {
         A.out[0] = u.d_prev;
         A.dtf = dt;
         if ((rc = P.kern->launch(S, nullptr)) != PHIX_OK) throw std::runtime_error("Solver: fused Euler launch failed");
+    } else if (S.pattern == fuse::PATTERN_COMPOSITE && S.dim == 2 && phix::step_pair_supported(A.L, 2)) {
+        // the whole RK4 step in one launch (the pair kernel, four periodic
+        // sides): the same operations per cell as the four stage launches
+        S.mode = phix::MODE_RK4_STEP;
+        A.out[0] = u.d_prev;
+        A.dtf = dt / 6.0;
+        S.dt_half = dt * 0.5;
+        S.dt_full = dt;
+        if ((rc = P.kern->launch(S, nullptr)) != PHIX_OK) throw std::runtime_error("Solver: fused RK4 step launch failed");
     } else {
         double* ks[3] = {k1_.d_curr, k2_.d_curr, k3_.d_curr};
         S.mode = phix::MODE_K;

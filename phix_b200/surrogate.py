@@ -437,11 +437,65 @@ def time_speed(params: np.ndarray, sur_steps: int = 40, n: int = N, warmup: int 
     return out
 
 
+def tradeoff(params: np.ndarray, seeds=(300, 301), fd_blocks=(0, 10, 50, 100, 200, 400, 600), total: int = 800,
+             n: int = N):
+    """The accuracy / speed trade-off of handing the first part of a run to
+    the FD solver.  For each held-out seed and each W in fd_blocks: the fused
+    FP64 FD solver advances the first W blocks (W * STEPS_PER_CALL steps), the
+    surrogate the remaining total - W blocks (with the mass projection); the
+    row reports rel-L2 against the pure FP64 FD state after `total` blocks,
+    and the speed-up of that schedule over pure FD from the measured device
+    times of one surrogate step and of one block of fused FD (FP32 and FP64).
+    Pure surrogate rollouts (W = 0) drift in the early linear regime of
+    spinodal decomposition, where differences grow exponentially; the rows
+    show how much of the run FD must cover for a given error."""
+    import torch
+    g = make_grid((n, n))
+    tm = time_speed(params, sur_steps=40, n=n)
+    per_sur = tm["surrogate_ms"] / 40.0
+    per_f32 = tm["fd_f32_ms"] / 40.0
+    per_f64 = tm["fd_f64_ms"] / 40.0
+    sg = Surrogate(n, n, 1, IN_SHIFT, IN_SCALE, OUT_SCALE)
+    sg.set_params(params)
+    plane = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    rows = []
+    for sd in seeds:
+        c0 = initial_field(sd, n)
+        st = Stepper(PHYS_CH, RK4, F64, PRM, DT, g)
+        d = torch.from_numpy(_stored(g, c0)).cuda()
+        st.load([d])
+        st.set_graph(STEPS_PER_CALL)
+        fd, done = {}, 0
+        for w in sorted(set(fd_blocks) | {total}):
+            st.advance((w - done) * STEPS_PER_CALL)
+            done = w
+            st.store([d])
+            plane_gather(d, plane, n, n, 1)
+            fd[w] = plane.clone()
+        st.close()
+        ref = fd[total]
+        for w in fd_blocks:
+            a = fd[w].clone()[None]
+            b = torch.empty_like(a)
+            for _ in range(total - w):
+                sg.step(a, b)
+                a, b = b, a
+            t_hyb64 = w * per_f64 + (total - w) * per_sur
+            t_hyb32 = w * per_f32 + (total - w) * per_sur
+            rows.append({"seed": sd, "fd_steps": w * STEPS_PER_CALL, "surrogate_steps": total - w,
+                         "rel_l2": _rel(a[0], ref), "rel_l2_fluct": _rel_fluct(a[0], ref),
+                         "mass_rel": abs(float(a[0].mean() - fd[0].mean())) / abs(float(fd[0].mean())),
+                         "speedup_vs_fd_f64": total * per_f64 / t_hyb64,
+                         "speedup_vs_fd_f32": total * per_f32 / t_hyb32})
+    sg.close()
+    return rows, tm
+
+
 def main(argv=None):
     import argparse
     import json
     ap = argparse.ArgumentParser(description="train / evaluate / time the CH 512^2 surrogate")
-    ap.add_argument("cmd", choices=["train", "evaluate", "time", "rollout"])
+    ap.add_argument("cmd", choices=["train", "evaluate", "time", "rollout", "tradeoff"])
     ap.add_argument("--steps", type=int, default=800, help="rollout: surrogate steps")
     ap.add_argument("--recheck", type=int, default=10, help="rollout: FD re-check every this many steps")
     ap.add_argument("--params", default=PARAMS_FILE)
@@ -501,6 +555,11 @@ def main(argv=None):
                                   / abs(float(c0.mean())), "surrogate_steps": rl.surrogate_steps,
                                   "fd_takeovers": rl.fd_takeovers, "rechecks": rl.rechecks,
                                   "rollout_s": rl.seconds, "fd_f64_s": fd_s}))
+        elif args.cmd == "tradeoff":
+            rows, tm = tradeoff(p, seeds=tuple(range(elo, ehi)))
+            print(json.dumps({"times_ms": tm}))
+            for r in rows:
+                print(json.dumps(r))
         else:
             print(json.dumps(time_speed(p)))
 

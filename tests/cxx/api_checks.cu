@@ -116,6 +116,52 @@ int main() {
             s.run(n);
         });
     }
+    // 2b. The same on four periodic sides: the one-launch RK4 step (pair
+    //     kernel through the user-functor policy) against the unfused path
+    {
+        Mesh mesh = Mesh::makeUniform2D(CoordSys::CARTESIAN, 200, 1.0, 0.0, 96, 0.9, 0.0);
+        fused_vs_unfused("CH 2-D RK4 composite, periodic (one launch per step)", mesh, 0.3, 0.7, 25,
+                         [&](ScalarField& c, bool fused, int n) {
+                             PeriodicBC bx(Axis::X), by(Axis::Y);
+                             std::vector<BoundaryCondition*> bcs = {&bx, &by};
+                             Equation eq(c, "ch");
+                             eq.setRHS(M * lap(pw(c, fprime) - kappa * lap(c), bcs));
+                             Solver s(eq, bcs, 0.004, TimeScheme::RK4);
+                             if (!fused) s.disableFusion();
+                             s.run(n);
+                         });
+    }
+    // 2c. Time of the C++ Solver::advance on CH 1024^2 RK4 (four periodic
+    //     sides, FP64): one launch per step
+    {
+        Mesh mesh = Mesh::makeUniform2D(CoordSys::CARTESIAN, 1024, 1.0, 0.0, 1024, 1.0, 0.0);
+        ScalarField c(mesh, "c");
+        fill_random(c, 0.49, 0.51, 3);
+        c.allocDevice();
+        c.uploadAllToDevice();
+        PeriodicBC bx(Axis::X), by(Axis::Y);
+        std::vector<BoundaryCondition*> bcs = {&bx, &by};
+        Equation eq(c, "ch");
+        eq.setRHS(M * lap(pw(c, fprime) - kappa * lap(c), bcs));
+        Solver s(eq, bcs, 0.005, TimeScheme::RK4);
+        s.run(20);
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        const int nrun = 400;
+        cudaEventRecord(e0);
+        for (int i = 0; i < nrun; ++i) s.advance();
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "CH 1024^2 RK4 FP64 through Solver::advance: %.2f us per step (%d steps)",
+                      1e3 * ms / nrun, nrun);
+        report("C++ Solver one-launch RK4 timing", s.fused() && ms > 0.f, buf);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
     // 3. Multi-step Cahn-Hilliard (mu STEADY, c TRANSIENT), Euler, periodic
     {
         Mesh mesh = Mesh::makeUniform2D(CoordSys::CARTESIAN, 100, 1.0, 0.0, 61, 1.0, 0.0);

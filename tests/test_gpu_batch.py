@@ -125,3 +125,41 @@ def test_batch_one_launch_step_needs_periodic_or_noflux_sides(cuda):
     b.set_fusion(False)
     assert b.launches_per_step == 4
     b.close()
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32])
+def test_batch_temporal_blocking_depth2(cuda, prec):
+    """Two RK4 steps per launch over the whole batch (pair kernels, every
+    instance periodic) give each instance the bits of the single-field
+    stepper, with an odd step count and graph replay."""
+    grids, phys, prms, scheme, dt, fields = small_batch(prec)
+    grids[1] = px.make_grid((40, 40))
+    b = px.Batch(phys, scheme, prec, grids, prms, dt)
+    b.set_fusion(True)
+    b.set_depth(2)
+    assert b.depth == 2
+    for i, f in enumerate(fields):
+        b.load(i, f)
+    b.set_graph(4)
+    nsteps = 9
+    before = px.launch_count()
+    b.advance(nsteps)
+    torch.cuda.synchronize()
+    assert px.launch_count() - before == nsteps // 2 + 1
+    for i, (g, prm, f) in enumerate(zip(grids, prms, fields)):
+        out = np.empty_like(f)
+        b.store(i, out)
+        want = single(g, phys, prm, scheme, dt, f, nsteps, prec)
+        gh = g.ghost
+        sl = (slice(gh, gh + g.n[2]), slice(gh, gh + g.n[1]), slice(gh, gh + g.n[0]))
+        assert np.array_equal(out[sl], want[sl]), i
+    b.close()
+
+
+def test_batch_depth2_needs_the_pair_kernels(cuda):
+    grids, phys, prms, scheme, dt, fields = small_batch(px.F32)  # one zero-flux instance
+    b = px.Batch(phys, scheme, px.F32, grids, prms, dt)
+    with pytest.raises(px.PhixError):
+        b.set_depth(2)
+    assert b.depth == 1
+    b.close()

@@ -19,6 +19,15 @@ write the same fields bit for bit.
     as one fused launch per step here; its files must equal the reference's
     byte for byte.
 
+  * applications/solvers/Cahn-Hillard+Allen-Cahn_double-well/2D: the coupled
+    CH+AC application (three SolverSteps: mu STEADY from pw of c and of eta
+    and lap c; c and eta TRANSIENT), all files equal the reference's.
+  * develop/Spinodal Decomposition/Cahn-Hillard.cu and
+    develop/Ostwald_Ripening/AC-CH.cu: the develop drivers' manual loops
+    (BCs by applyOnGPU, Equation::computeRHS called directly, single-equation
+    Euler Solvers on other fields).  They run 1e8 steps; the test stops each
+    after its step-10000 output and compares every file written up to then.
+
 The binaries are built where the reference tree exists; without them the
 tests skip.
 """
@@ -210,3 +219,90 @@ def test_gfa_app_identical(cuda, tmp_path):
     for n in names:
         assert files["ours"][n] == files["ref"][n], f"{n}: differs from the reference (field max-abs {worst:.3e})"
     print(f"GFA app: {len(names)} files identical to the reference's")
+
+
+CHAC_SETTINGS = """{{
+    // written by tests/test_gpu_dropin.py
+    "mesh": {{"nx": {nx}, "ny": {ny}, "dx": 1.0, "dy": 1.0, "x0": 0.0, "y0": 0.0}},
+    "initialize": {{"start_from": "initial_field", "dt": 0.005, "nSteps": {nsteps}}},
+    "boundary_conditions": {{"x_min": "Periodic", "x_max": "Periodic", "y_min": "NoFlux", "y_max": "NoFlux"}},
+    "constants": {{"rho": 1.4142135623730951, "ca": 0.3, "cb": 0.7, "kappa_c": 3.0, "kappa_eta": 3.0,
+                   "M": 5.0, "L": 5.0, "w": 1.0}},
+    "output": {{"print_interval": {every}, "write_interval": {every}, "format": "ALL"}}
+}}
+"""
+
+
+def test_chac_app_identical(cuda, tmp_path):
+    exes = {"ref": _bin("chacapp_ref"), "ours": _bin("chacapp_phix")}
+    nx, ny, nsteps, every = 128, 96, 600, 200
+    rng = np.random.default_rng(6)
+    c0 = 0.5 + rng.uniform(-0.05, 0.05, size=(ny, nx))
+    eta0 = rng.uniform(0.0, 0.1, size=(ny, nx))
+    out, files = {}, {}
+    for tag, exe in exes.items():
+        d = tmp_path / tag
+        (d / "settings" / "initial_field").mkdir(parents=True)
+        (d / "settings" / "settings.jsonc").write_text(CHAC_SETTINGS.format(nx=nx, ny=ny, nsteps=nsteps, every=every))
+        for name, a in (("c", c0), ("eta", eta0), ("mu", np.zeros_like(c0))):
+            _write_field(d / "settings" / "initial_field" / f"{name}.field", name, a)
+        rc, text = _run(exe, d)
+        assert rc == 0, text[-2000:]
+        out[tag] = [l for l in text.splitlines() if "written:" in l]
+        files[tag] = {n: (d / "output" / n).read_bytes() for n in sorted(os.listdir(d / "output"))}
+    names = sorted(files["ref"])
+    assert sorted(files["ours"]) == names and len(names) == 2 * 3 * (nsteps // every + 1)
+    assert out["ours"] == out["ref"]
+    for n in names:
+        if n.endswith(".field") and files["ours"][n] != files["ref"][n]:
+            a, b = files["ref"][n], files["ours"][n]
+            cut = a.index(b"---\n") + 4
+            da, db = np.frombuffer(a[cut:], "<f8"), np.frombuffer(b[cut:], "<f8")
+            pytest.fail(f"{n}: max-abs {np.abs(da - db).max():.3e} against the reference")
+        assert files["ours"][n] == files["ref"][n], n
+    print(f"CH+AC app: {len(names)} files identical to the reference's")
+
+
+def _run_until(binary, cwd, marker, timeout=600):
+    """Runs a driver until a line containing `marker` is printed, then stops
+    it (the develop drivers loop for 1e8 steps); returns the printed lines."""
+    import time
+    p = subprocess.Popen([binary], cwd=cwd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    lines, t0 = [], time.time()
+    try:
+        for line in p.stdout:
+            lines.append(line.rstrip("\n"))
+            if marker in line or time.time() - t0 > timeout:
+                break
+    finally:
+        p.terminate()
+        try:
+            p.wait(timeout=60)
+        except subprocess.TimeoutExpired:
+            p.kill()
+            p.wait()
+    return lines
+
+
+@pytest.mark.parametrize("driver,marker", [("devch", "written: output/c_10000.field"),
+                                           ("ostwald", "written: output/eta_10000.field")])
+def test_develop_manual_loop_drivers_identical(cuda, tmp_path, driver, marker):
+    logs, files = {}, {}
+    for tag in ("ref", "phix"):
+        d = tmp_path / tag
+        d.mkdir()
+        lines = _run_until(_bin(f"{driver}_{tag}"), d, marker)
+        assert any(marker in l for l in lines), "\n".join(lines[-20:])
+        logs[tag] = [l for l in lines if "written:" in l or "progress" in l]
+        files[tag] = {n: (d / "output" / n).read_bytes() for n in sorted(os.listdir(d / "output"))}
+    assert logs["phix"] == logs["ref"]
+    names = [n for n in sorted(files["ref"]) if int(n.split("_")[1].split(".")[0]) <= 10000]
+    assert len(names) >= (4 if driver == "devch" else 8)
+    for n in names:
+        a, b = files["ref"][n], files["phix"].get(n)
+        assert b is not None, n
+        if a != b:
+            cut = a.index(b"---\n") + 4
+            da, db = np.frombuffer(a[cut:], "<f8"), np.frombuffer(b[cut:], "<f8")
+            pytest.fail(f"{driver} {n}: max-abs {np.abs(da - db).max():.3e} against the reference")
+    print(f"{driver}: {len(names)} files identical to the reference's")

@@ -177,9 +177,11 @@ FUSED_CASES = [
 ]
 
 # one-launch step tiles: 0-5 the box kernel, 6-15 the pair kernel (CH with
-# four periodic sides); those that do not fit in shared memory per precision
-STEP_TILES = {px.F64: (0, 1, 2, 3, 7, 8, 9, 10, 11, 13, 14, 15), px.F32: tuple(range(16))}
-PAIR_TILES = set(range(6, 16))
+# four periodic sides), 16-19 the pair kernel two steps per launch; those
+# that do not fit in shared memory per precision
+STEP_TILES = {px.F64: (0, 1, 2, 3, 7, 8, 9, 10, 11, 13, 14, 15, 16, 17, 18, 19), px.F32: tuple(range(20))}
+PAIR_TILES = set(range(6, 20))
+DEPTH2_TILES = set(range(16, 20))
 
 
 @pytest.mark.parametrize("prec", [px.F64, px.F32])
@@ -468,3 +470,44 @@ def test_autotune_restores_state_and_keeps_bits(cuda, prec):
     keep = ~corner_mask(grid)
     assert np.array_equal(loaded[0][keep], loaded[1][keep])
     assert np.array_equal(outs[0][keep], outs[1][keep]), _where(outs[1], outs[0], keep)
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32])
+@pytest.mark.parametrize("tile", sorted(DEPTH2_TILES))
+@pytest.mark.parametrize("nsteps,graph", [(11, 0), (12, 5), (9, 4)])
+def test_temporal_blocking_depth2_matches_single_steps(cuda, oracle, prec, tile, nsteps, graph):
+    """Two RK4 steps per launch (the first step's update kept in shared
+    memory on the tile + 8) give the bits of one launch per step, for odd
+    step counts (a single-step launch finishes), graph groups of either
+    parity, partial tiles and grids smaller than the 16-cell halo; the ghost
+    faces equal the single-step path's."""
+    n = (150, 37) if tile != 19 else (13, 20)
+    g = px.make_grid(n, (1.0, 0.9), 1)
+    grid = Grid(n=n, d=(1.0, 0.9))
+    rng = np.random.default_rng(7 + tile)
+    x = grid.stored_from_phys(rng.uniform(0.3, 0.7, size=(1, n[1], n[0])))
+    prm = [1.0, 0.6, 1.2, 0.05, 0.95]
+    outs = []
+    for t in (tile, -1):
+        st = px.Stepper(px.PHYS_CH, px.RK4, prec, prm, 0.004, g)
+        st.set_tiles(t)
+        assert st.depth == (2 if t == tile else 1)
+        d = torch.from_numpy(x.copy()).cuda()
+        st.load([d])
+        st.set_graph(graph)
+        before = px.launch_count()
+        st.advance(nsteps)
+        torch.cuda.synchronize()
+        launches = px.launch_count() - before
+        st.store([d])
+        torch.cuda.synchronize()
+        st.close()
+        outs.append(d.cpu().numpy())
+        if t == tile:
+            assert launches == nsteps // 2 + nsteps % 2
+    keep = ~corner_mask(grid)
+    assert np.array_equal(outs[0][keep], outs[1][keep])
+    if prec == px.F64:
+        want = [x.copy()]
+        oracle.advance(want, px.PHYS_CH, prm, px.RK4, 0.004, nsteps, grid, fma_mode=1)
+        assert np.array_equal(outs[0][keep], want[0][keep])
