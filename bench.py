@@ -246,7 +246,7 @@ class StepperRun:
         if args.autotune:
             self.st.autotune(10)  # launch form and tile shape, timed on this grid (state restored)
         fused, tile = self.st.tiles()
-        self.launch = {"one_launch_per_time_step": fused, "tile_cfg": tile}
+        self.launch = {"one_launch_per_time_step": fused, "tile_cfg": tile, "temporal_depth": self.st.depth}
         self.lps = self.st.launches_per_step
         self.kernel = dominant_kernel(px, g, phys, scheme, self.lps, fused, tile)
         self.st.set_graph(self.K)
@@ -301,6 +301,7 @@ class BatchRun:
             if args.launch == "stage":
                 self.b.set_fusion(False)
         self.lps = self.b.launches_per_step
+        self.launch = {"temporal_depth": self.b.depth}
         periodic = all(g.bc_type[i] == px.BC_PERIODIC for g in grids for i in range(4))
         self.kernel = ("step_pair_batched" if periodic and phys == px.PHYS_CH else "step_box_batched") \
             if self.lps == 1 else "stage_box_batched"

@@ -76,6 +76,22 @@ __global__ void __launch_bounds__(256) f32_rows_to_f64(double* __restrict__ x, c
     }
 }
 
+// FP64 copies between the callers' layout (pitch sx) and a row-padded one (pk).
+__global__ void __launch_bounds__(256) f64_rows_to_padded(double* __restrict__ dst, const double* __restrict__ src,
+                                                          size_t n, int sx, int pk) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / (size_t)sx;
+        dst[r * pk + (i - r * sx)] = src[i];
+    }
+}
+__global__ void __launch_bounds__(256) f64_rows_from_padded(double* __restrict__ dst, const double* __restrict__ src,
+                                                            size_t n, int sx, int pk) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / (size_t)sx;
+        dst[i] = src[r * pk + (i - r * sx)];
+    }
+}
+
 static int aligned16(const void* a, const void* b) {
     return ((uintptr_t)a % 16 == 0) && ((uintptr_t)b % 16 == 0);
 }
@@ -121,7 +137,10 @@ int stepper_copy_in(phix_stepper* h, const double* const* fields, cudaStream_t s
         const int sx = stepper_grid_layout(h).s[1], pk = stepper_layout(h).s[1];
         for (int b = 0; b < nb; ++b) {
             void* dst = stepper_state_buf(h, b, f);
-            if (pk != sx) {  // row-padded FP32 state
+            if (pk != sx && stepper_prec(h) == PHIX_F64) {  // row-padded FP64 state
+                f64_rows_to_padded<<<conv_grid(S), 256, 0, s>>>((double*)dst, fields[f], S, sx, pk);
+                PHIX_LAUNCH_CHECK("f64_rows_to_padded");
+            } else if (pk != sx) {  // row-padded FP32 state
                 f64_split_f32_rows<<<conv_grid(S), 256, 0, s>>>((float*)dst, (float*)stepper_lo_buf(h, b, f), fields[f],
                                                                 S, sx, pk);
                 PHIX_LAUNCH_CHECK("f64_split_f32_rows");
@@ -147,7 +166,10 @@ int stepper_copy_out(phix_stepper* h, double* const* fields, cudaStream_t s) {
         if (!fields[f]) { set_error("store: field %d is NULL", f); return PHIX_ERR_ARG; }
         const void* src = stepper_state(h, f);
         const int sx = stepper_grid_layout(h).s[1], pk = stepper_layout(h).s[1];
-        if (pk != sx) {  // row-padded FP32 state
+        if (pk != sx && stepper_prec(h) == PHIX_F64) {  // row-padded FP64 state
+            f64_rows_from_padded<<<conv_grid(S), 256, 0, s>>>(fields[f], (const double*)src, S, sx, pk);
+            PHIX_LAUNCH_CHECK("f64_rows_from_padded");
+        } else if (pk != sx) {  // row-padded FP32 state
             const bool multi_mu = stepper_scheme(h) == PHIX_MULTISTEP && f == 1;
             const void* lo = multi_mu ? nullptr : stepper_lo_buf(h, stepper_cur(h), f);
             f32_rows_to_f64<<<conv_grid(S), 256, 0, s>>>(fields[f], (const float*)src, (const float*)lo, S, sx, pk);
@@ -175,8 +197,9 @@ int stepper_diag(phix_stepper* h, double* out) {
     const int np = reduce_partials_needed(stepper_grid(h));
     double* part = stepper_partials(h, np);
     if (!part) { set_error("diagnostics: cudaMalloc failed"); return PHIX_ERR_CUDA; }
-    if (stepper_prec(h) == PHIX_F32) {
-        // FP64 value of the compensated state (hi + lo) in the staging buffer
+    if (stepper_prec(h) == PHIX_F32 || stepper_layout(h).s[1] != stepper_grid_layout(h).s[1]) {
+        // FP64 value of the compensated state (hi + lo), or of a row-padded
+        // FP64 state, in the grid's layout in the staging buffer
         double* stage = stepper_staging(h);
         if (!stage) { set_error("diagnostics: cudaMalloc(staging) failed"); return PHIX_ERR_CUDA; }
         const size_t S = stepper_stored(h);

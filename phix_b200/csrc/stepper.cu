@@ -910,13 +910,14 @@ int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precisio
     h->L = L;
     h->S = S;
     h->esz = precision == PHIX_F32 ? 4 : 8;
-    // 3-D FP32 steppers keep their arrays with rows padded to whole 16-byte
+    // 3-D steppers keep their own arrays with rows padded to whole 16-byte
     // units (a TMA row stride must be one); the ghost layers stay where the
     // layout's origin puts them, the padding columns are never read
     h->Lk = L;
     h->Sk = S;
-    if (precision == PHIX_F32 && g->dim == 3) {
-        const int sx = L.s[1], pk = (sx + 3) / 4 * 4, sy = L.s[2] / L.s[1], gh = L.ghost;
+    if (g->dim == 3) {
+        const int vec = 16 / (int)h->esz;
+        const int sx = L.s[1], pk = (sx + vec - 1) / vec * vec, sy = L.s[2] / L.s[1], gh = L.ghost;
         h->Lk.s[1] = pk;
         h->Lk.s[2] = pk * sy;
         h->Lk.origin = gh + pk * (gh + sy * gh);
@@ -1143,6 +1144,7 @@ int phix_stepper_bind(phix_stepper_t* h, double* const* fields, double* const* a
             for (auto& p : b)
                 if (p) { cudaFree(p); p = nullptr; }
     h->own_state = false;
+    h->Lk = h->L;  // the callers' arrays have the grid's own layout (k buffers are large enough for it)
     for (int f = 0; f < h->nf; ++f) {
         h->st[0][f] = fields[f];
         h->st[1][f] = alt[f] ? alt[f] : fields[f];

@@ -437,18 +437,19 @@ def time_speed(params: np.ndarray, sur_steps: int = 40, n: int = N, warmup: int 
     return out
 
 
-def tradeoff(params: np.ndarray, seeds=(300, 301), fd_blocks=(0, 10, 50, 100, 200, 400, 600), total: int = 800,
-             n: int = N):
-    """The accuracy / speed trade-off of handing the first part of a run to
-    the FD solver.  For each held-out seed and each W in fd_blocks: the fused
-    FP64 FD solver advances the first W blocks (W * STEPS_PER_CALL steps), the
-    surrogate the remaining total - W blocks (with the mass projection); the
-    row reports rel-L2 against the pure FP64 FD state after `total` blocks,
-    and the speed-up of that schedule over pure FD from the measured device
-    times of one surrogate step and of one block of fused FD (FP32 and FP64).
-    Pure surrogate rollouts (W = 0) drift in the early linear regime of
-    spinodal decomposition, where differences grow exponentially; the rows
-    show how much of the run FD must cover for a given error."""
+def tradeoff(params: np.ndarray, seeds=(300, 301), fd_blocks=(0, 10, 50, 100, 200, 400, 600),
+             fd_every=(0, 10, 4), total: int = 800, n: int = N):
+    """The accuracy / speed trade-off of handing part of a run to the FD
+    solver.  For each held-out seed, each W in fd_blocks and each R in
+    fd_every: the fused FP64 FD solver advances the first W blocks
+    (W * STEPS_PER_CALL steps), and after that every R-th block (R = 0: none);
+    the surrogate (with the mass projection) advances the other blocks.  Each
+    row reports rel-L2 against the pure FP64 FD state after `total` blocks and
+    the schedule's speed-up over pure FD, from the measured device times of
+    one surrogate step and of one block of fused FD (FP32 and FP64).  Pure
+    surrogate rollouts drift in the early linear regime of spinodal
+    decomposition, where differences grow exponentially; the rows show how
+    much of the run FD must cover for a given error."""
     import torch
     g = make_grid((n, n))
     tm = time_speed(params, sur_steps=40, n=n)
@@ -458,13 +459,14 @@ def tradeoff(params: np.ndarray, seeds=(300, 301), fd_blocks=(0, 10, 50, 100, 20
     sg = Surrogate(n, n, 1, IN_SHIFT, IN_SCALE, OUT_SCALE)
     sg.set_params(params)
     plane = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    st = Stepper(PHYS_CH, RK4, F64, PRM, DT, g)
+    st.set_graph(STEPS_PER_CALL)
+    d = torch.empty(stored_shape(g), dtype=torch.float64, device="cuda")
     rows = []
     for sd in seeds:
         c0 = initial_field(sd, n)
-        st = Stepper(PHYS_CH, RK4, F64, PRM, DT, g)
-        d = torch.from_numpy(_stored(g, c0)).cuda()
+        d.copy_(torch.from_numpy(_stored(g, c0)))
         st.load([d])
-        st.set_graph(STEPS_PER_CALL)
         fd, done = {}, 0
         for w in sorted(set(fd_blocks) | {total}):
             st.advance((w - done) * STEPS_PER_CALL)
@@ -472,21 +474,35 @@ def tradeoff(params: np.ndarray, seeds=(300, 301), fd_blocks=(0, 10, 50, 100, 20
             st.store([d])
             plane_gather(d, plane, n, n, 1)
             fd[w] = plane.clone()
-        st.close()
         ref = fd[total]
         for w in fd_blocks:
-            a = fd[w].clone()[None]
-            b = torch.empty_like(a)
-            for _ in range(total - w):
-                sg.step(a, b)
-                a, b = b, a
-            t_hyb64 = w * per_f64 + (total - w) * per_sur
-            t_hyb32 = w * per_f32 + (total - w) * per_sur
-            rows.append({"seed": sd, "fd_steps": w * STEPS_PER_CALL, "surrogate_steps": total - w,
-                         "rel_l2": _rel(a[0], ref), "rel_l2_fluct": _rel_fluct(a[0], ref),
-                         "mass_rel": abs(float(a[0].mean() - fd[0].mean())) / abs(float(fd[0].mean())),
-                         "speedup_vs_fd_f64": total * per_f64 / t_hyb64,
-                         "speedup_vs_fd_f32": total * per_f32 / t_hyb32})
+            for r in fd_every:
+                a = fd[w].clone()[None]
+                b = torch.empty_like(a)
+                nfd = 0
+                for k in range(w, total):
+                    if r and (k - w) % r == r - 1:  # this block by FD
+                        plane_scatter(a[0], d, n, n, 1)
+                        st.load([d])
+                        st.advance(STEPS_PER_CALL)
+                        st.store([d])
+                        plane_gather(d, a[0], n, n, 1)
+                        nfd += 1
+                    else:
+                        sg.step(a, b)
+                        a, b = b, a
+                nsur = total - w - nfd
+                t64 = (w + nfd) * per_f64 + nsur * per_sur
+                t32 = (w + nfd) * per_f32 + nsur * per_sur
+                rows.append({"seed": sd, "fd_warmup_steps": w * STEPS_PER_CALL, "fd_every": r,
+                             "fd_blocks": w + nfd, "surrogate_steps": nsur,
+                             "rel_l2": _rel(a[0], ref), "rel_l2_fluct": _rel_fluct(a[0], ref),
+                             "mass_rel": abs(float(a[0].mean() - fd[0].mean())) / abs(float(fd[0].mean())),
+                             "speedup_vs_fd_f64": total * per_f64 / t64,
+                             "speedup_vs_fd_f32": total * per_f32 / t32})
+                if w == total:
+                    break
+    st.close()
     sg.close()
     return rows, tm
 

@@ -67,7 +67,7 @@ def test_fused_3d_step_matches_per_stage_launches(cuda, oracle, prec, case):
     fields = _inputs(phys, n, grid, hash(n) % 1000)
     fused, lps_f = _run(phys, g, prec, fields, True)
     staged, lps_s = _run(phys, g, prec, fields, False)
-    assert lps_f == 2 and lps_s == 4
+    assert lps_f == 2 and lps_s == 4  # odd FP64 rows too: the stepper's own arrays are row-padded
     for a, b in zip(fused, staged):
         pa, pb = grid.phys(a), grid.phys(b)
         bad = np.argwhere(pa != pb)
@@ -97,3 +97,28 @@ def test_fused_3d_graph_replay_and_ghosts(cuda, oracle):
     faces[:, 1:-1, 1:-1] = True
     for x, y in zip(a, b):
         assert np.array_equal(x[faces], y[faces])
+
+
+def test_fused_3d_on_bound_buffers_with_odd_rows_falls_back(cuda):
+    """Caller-owned FP64 buffers keep the grid's layout: rows of 39 doubles
+    are not whole 16-byte units, so the step runs one launch per stage (same
+    bits); an even row length keeps the fused path."""
+    for n0, want in ((37, 4), (38, 2)):
+        n = (n0, 20, 12)
+        bcs = (px.BC_NOFLUX, px.BC_NOFLUX) + (px.BC_PERIODIC,) * 4
+        g = px.make_grid(n, (1.0, 1.0, 1.0), 1, bcs)
+        grid = Grid(n=n, bc=bcs)
+        fields = _inputs(px.PHYS_CHAC, n, grid, 3)
+        st = px.Stepper(px.PHYS_CHAC, px.RK4, px.F64, PRM[px.PHYS_CHAC], DT[px.PHYS_CHAC], g)
+        d = [torch.from_numpy(f.copy()).cuda() for f in fields]
+        alt = [x.clone() for x in d]
+        st.bind(d, alt)
+        assert st.launches_per_step == want
+        st.advance(4)
+        torch.cuda.synchronize()
+        st.status()
+        got = [(alt if st.current() else d)[f].cpu().numpy() for f in range(2)]
+        st.close()
+        ref, _ = _run(px.PHYS_CHAC, g, px.F64, fields, False, nsteps=4)
+        for a, b in zip(got, ref):
+            assert np.array_equal(grid.phys(a), grid.phys(b))
