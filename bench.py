@@ -203,7 +203,9 @@ def dominant_kernel(px, g, phys, scheme, lps, fused, tile):
     """Name of the kernel that takes the time step (the key of TRAFFIC)."""
     periodic_ch = phys == px.PHYS_CH and g.dim == 2 and all(g.bc_type[i] == px.BC_PERIODIC for i in range(4))
     if g.dim == 3:
-        return "stage2_march3d" if lps == 2 else "stage_march3d"
+        if lps == 2:
+            return "stage2_march3d"
+        return "stage_march3d" if tile == 2 or phys == px.PHYS_AC else "stage_stream3d"
     if scheme == px.MULTISTEP:
         return "step_pair_ms" if fused else "stage_box"
     if lps == 1 and scheme == px.RK4 and fused:

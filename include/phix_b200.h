@@ -201,7 +201,12 @@ int phix_stepper_depth(const phix_stepper_t* h);
  * shared memory for the precision are refused when the step runs.
  * PHIX_MULTISTEP steppers with the pair-layout step: 0..5 pair tiles of
  * 128x32, 64x32, 128x16, 64x16, 64x64, 256x16 with 8, 8, 4, 4, 8, 4 row
- * blocks (threads = (TX/2 + 2) x row blocks).  -1 picks by grid (see
+ * blocks (threads = (TX/2 + 2) x row blocks).  3-D steppers: with one launch
+ * per stage, -1 streams CH / CH+AC grids (z periodic; x, y periodic or
+ * zero-flux) through the TMA-staged kernel and 2 selects the marching kernel
+ * without TMA; on the fused two-stage RK4 path 0 (the default) or 1 pick two
+ * tile variants (the second puts the stages-3-4 launch on 32x8 tiles).  -1
+ * picks by grid (see
  * phix_stepper_autotune for a measured choice).  All give the same bits.
  * No reference counterpart. */
 int phix_stepper_set_tiles(phix_stepper_t* h, int tile_cfg);

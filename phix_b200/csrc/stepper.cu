@@ -24,6 +24,7 @@
 #include "phix/detail/step2d_pair.cuh"
 #include "phix/detail/step2d_pair_ms.cuh"
 #include "phix/detail/march3d_fused.cuh"
+#include "phix/detail/stream3d.cuh"
 #include "stepper.h"
 
 #include <cudaTypedefs.h>
@@ -590,15 +591,23 @@ namespace phix {
 // ---------------------------------------------------------------------------
 namespace {
 
-// tiles (TX, TY, threads) of launch A (stages 1-2) and launch B (stages 3-4):
-// the largest that keep two CTAs per SM for FP32 A (113 KB of shared memory)
-// and fit one CTA per SM otherwise
-template <typename T> struct M2Cfg;
-template <> struct M2Cfg<float> {
+// tiles (TX, TY, threads) of launch A (stages 1-2) and launch B (stages 3-4),
+// two variants per precision (phix_stepper_set_tiles 0 / 1 on 3-D grids, -1 =
+// 0).  Variant 0: the largest tiles (FP32 A 113 KB of shared memory, two CTAs
+// per SM; B 173 KB, one); variant 1: B at 32x8 (FP32 113 KB, two CTAs per SM)
+// and, in FP64, A at 32x8 too.
+template <typename T, int V> struct M2Cfg;
+template <> struct M2Cfg<float, 0> {
     static constexpr int AX = 32, AY = 16, ANT = 256, BX = 32, BY = 16, BNT = 512;
 };
-template <> struct M2Cfg<double> {
+template <> struct M2Cfg<float, 1> {
+    static constexpr int AX = 32, AY = 16, ANT = 256, BX = 32, BY = 8, BNT = 256;
+};
+template <> struct M2Cfg<double, 0> {
     static constexpr int AX = 32, AY = 16, ANT = 512, BX = 32, BY = 8, BNT = 512;
+};
+template <> struct M2Cfg<double, 1> {
+    static constexpr int AX = 32, AY = 8, ANT = 256, BX = 32, BY = 8, BNT = 256;
 };
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -683,9 +692,9 @@ int m2_kernel(bool prepare, March2Args<T>* a, cudaStream_t s) {
     return PHIX_OK;
 }
 
-template <typename T, class Pol>
-int m2_step(bool prepare, March2Args<T>* a, cudaStream_t s, bool second) {
-    using C = M2Cfg<T>;
+template <typename T, class Pol, int V>
+int m2_step_v(bool prepare, March2Args<T>* a, cudaStream_t s, bool second) {
+    using C = M2Cfg<T, V>;
     if (prepare) {
         int rc = m2_kernel<T, Pol, C::AX, C::AY, C::ANT, false>(true, nullptr, s);
         return rc ? rc : m2_kernel<T, Pol, C::BX, C::BY, C::BNT, true>(true, nullptr, s);
@@ -694,31 +703,129 @@ int m2_step(bool prepare, March2Args<T>* a, cudaStream_t s, bool second) {
                   : m2_kernel<T, Pol, C::AX, C::AY, C::ANT, false>(false, a, s);
 }
 
+// variant < 0: prepare every variant (prepare) or run variant 0
+template <typename T, class Pol>
+int m2_step(bool prepare, March2Args<T>* a, cudaStream_t s, bool second, int variant) {
+    if (prepare) {
+        int rc = m2_step_v<T, Pol, 0>(true, a, s, second);
+        return rc ? rc : m2_step_v<T, Pol, 1>(true, a, s, second);
+    }
+    return variant == 1 ? m2_step_v<T, Pol, 1>(false, a, s, second) : m2_step_v<T, Pol, 0>(false, a, s, second);
+}
+
 template <typename T>
-int m2_dispatch(int phys, bool prepare, March2Args<T>* a, cudaStream_t s, bool second) {
-    if (phys == PHIX_PHYS_CH) return m2_step<T, PolCH>(prepare, a, s, second);
-    if (phys == PHIX_PHYS_CHAC) return m2_step<T, PolCHAC>(prepare, a, s, second);
+int m2_dispatch(int phys, bool prepare, March2Args<T>* a, cudaStream_t s, bool second, int variant = 0) {
+    if (variant > 1) {
+        set_error("fused 3-D step: tile variant %d (0 or 1)", variant);
+        return PHIX_ERR_UNSUPPORTED;
+    }
+    if (phys == PHIX_PHYS_CH) return m2_step<T, PolCH>(prepare, a, s, second, variant);
+    if (phys == PHIX_PHYS_CHAC) return m2_step<T, PolCHAC>(prepare, a, s, second, variant);
     set_error("fused 3-D step: physics %d has no chemical potential", phys);
+    return PHIX_ERR_UNSUPPORTED;
+}
+
+// ---- one stage of the mu physics streamed through z (stream3d.cuh) --------
+// tile per precision: TX x TY, (TX + 4) x (TY + 4) threads
+template <typename T> struct S3Cfg;
+template <> struct S3Cfg<float> { static constexpr int TX = 32, TY = 8; };
+template <> struct S3Cfg<double> { static constexpr int TX = 32, TY = 8; };
+
+template <typename T, class Pol, int MODE>
+int s3_kernel(bool prepare, Stream3Args<T>* a, cudaStream_t s) {
+    using C = S3Cfg<T>;
+    using G = Stream3<T, Pol, C::TX, C::TY>;
+    auto kern = stage_stream3d<T, Pol, MODE, C::TX, C::TY>;
+    if (prepare) {
+        PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
+        return PHIX_OK;
+    }
+    static int slots = 0;  // resident CTAs on the device
+    if (!slots) {
+        int dev = 0, nsm = 0, occ = 0;
+        PHIX_TRY_CUDA(cudaGetDevice(&dev));
+        PHIX_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        PHIX_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, G::NT, G::smem_bytes()));
+        slots = (occ > 0 ? occ : 1) * nsm;
+    }
+    const Layout& L = a->S.L;
+    int rc;
+    for (int f = 0; f < G::NF; ++f) {
+        if ((rc = plane_map(&a->tu[f], a->S.u[f], L, (int)sizeof(T), G::WB, G::HB))) return rc;
+        if (a->S.kin[0] && (rc = plane_map(&a->tk[f], a->S.kin[f], L, (int)sizeof(T), G::WB, G::HB))) return rc;
+    }
+    const long long cols = (long long)((L.n[0] + C::TX - 1) / C::TX) * ((L.n[1] + C::TY - 1) / C::TY);
+    a->rz = pick_rz(cols, L.n[2], slots, G::H);
+    dim3 grid((L.n[0] + C::TX - 1) / C::TX, (L.n[1] + C::TY - 1) / C::TY, (L.n[2] + a->rz - 1) / a->rz);
+    kern<<<grid, G::NT, G::smem_bytes(), s>>>(*a);
+    PHIX_LAUNCH_CHECK("stage_stream3d");
+    return PHIX_OK;
+}
+
+template <typename T, class Pol>
+int s3_mode(int mode, bool prepare, Stream3Args<T>* a, cudaStream_t s) {
+    if (prepare) {
+        int rc = s3_kernel<T, Pol, MODE_K>(true, a, s);
+        if (!rc) rc = s3_kernel<T, Pol, MODE_RK4_FINAL>(true, a, s);
+        return rc ? rc : s3_kernel<T, Pol, MODE_EULER_FINAL>(true, a, s);
+    }
+    switch (mode) {
+        case MODE_K: return s3_kernel<T, Pol, MODE_K>(false, a, s);
+        case MODE_RK4_FINAL: return s3_kernel<T, Pol, MODE_RK4_FINAL>(false, a, s);
+        case MODE_EULER_FINAL: return s3_kernel<T, Pol, MODE_EULER_FINAL>(false, a, s);
+    }
+    set_error("stage_stream3d: mode %d", mode);
+    return PHIX_ERR_UNSUPPORTED;
+}
+
+template <typename T>
+int s3_dispatch(int phys, int mode, bool prepare, Stream3Args<T>* a, cudaStream_t s) {
+    if (phys == PHIX_PHYS_CH) return s3_mode<T, PolCH>(mode, prepare, a, s);
+    if (phys == PHIX_PHYS_CHAC) return s3_mode<T, PolCHAC>(mode, prepare, a, s);
+    set_error("stage_stream3d: physics %d has no chemical potential", phys);
     return PHIX_ERR_UNSUPPORTED;
 }
 
 }  // namespace
 
-// The fused 3-D path takes the grid: RK4 of CH or CH+AC, z periodic, x and y
-// periodic or zero-flux, rows of whole 16-byte units, 16-byte aligned arrays.
-static bool step3d_fused(const phix_stepper* h) {
-    if (!h->fuse_steps || !h->fuse3d || h->scheme != PHIX_RK4 || h->dim != 3) return false;
-    if (h->phys != PHIX_PHYS_CH && h->phys != PHIX_PHYS_CHAC) return false;
+// The 3-D stage kernels with TMA plane staging take the grid: CH or CH+AC,
+// z periodic, x and y periodic or zero-flux, rows of whole 16-byte units,
+// 16-byte aligned arrays (the stepper's own arrays are row-padded).
+static bool tma3d_ok(const phix_stepper* h) {
+    if (h->dim != 3 || (h->phys != PHIX_PHYS_CH && h->phys != PHIX_PHYS_CHAC)) return false;
     const Layout& L = h->Lk;
     for (int i = 0; i < 4; ++i)
         if (L.bc[i] != PHIX_BC_PERIODIC && L.bc[i] != PHIX_BC_NOFLUX) return false;
     if (L.bc[4] != PHIX_BC_PERIODIC) return false;
     if ((L.s[1] * h->esz) % 16 != 0) return false;
-    const int nfb = h->nf;
-    for (int f = 0; f < nfb; ++f)
+    for (int f = 0; f < h->nf; ++f)
         for (int b = 0; b < 2; ++b)
             if ((uintptr_t)h->st[b][f] % 16 != 0) return false;
     return tensor_map_encoder() != nullptr;
+}
+
+// Tile configuration of 3-D steppers that selects the marching stage kernel
+// (no TMA) for one launch per stage.
+constexpr int TILE3D_MARCH = 2;
+
+// One 3-D stage: streamed with TMA staging where tma3d_ok (unless the tile
+// configuration asks for the marching kernel), else stage_march3d.
+template <typename T>
+static int launch_stage3d(const phix_stepper* h, int mode, const StageArgs<T>& A, cudaStream_t s) {
+    if (h->dim == 3 && h->tile != TILE3D_MARCH && tma3d_ok(h)) {
+        Stream3Args<T> a;
+        memset(&a, 0, sizeof(a));
+        a.S = A;
+        a.err = h->err;
+        return s3_dispatch<T>(h->phys, mode, false, &a, s);
+    }
+    return launch_stage<T>(h->phys, h->dim, mode, A, s, h->tile);
+}
+
+// The fused 3-D path takes the grid: RK4 of CH or CH+AC, z periodic, x and y
+// periodic or zero-flux, rows of whole 16-byte units, 16-byte aligned arrays.
+static bool step3d_fused(const phix_stepper* h) {
+    return h->fuse_steps && h->fuse3d && h->scheme == PHIX_RK4 && tma3d_ok(h);
 }
 
 static void drop_graphs(phix_stepper* h) {
@@ -771,7 +878,7 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s, int depth) {
         for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->st[o][f];
         A.dtf = (T)h->dt;
         set_lo(h->nf);
-        rc = launch_stage<T>(h->phys, h->dim, MODE_EULER_FINAL, A, s, h->tile);
+        rc = launch_stage3d<T>(h, MODE_EULER_FINAL, A, s);
         if (rc) return rc;
     } else if (step_fused(h)) {
         A.out[0] = (T*)h->st[o][0];
@@ -798,14 +905,14 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s, int depth) {
         M.err = h->err;
         M.a_in = dt2;
         M.a_mid = dt2;
-        if ((rc = m2_dispatch<T>(h->phys, false, &M, s, false))) return rc;
+        if ((rc = m2_dispatch<T>(h->phys, false, &M, s, false, h->tile))) return rc;
         M.a_mid = dtt;
-        if ((rc = m2_dispatch<T>(h->phys, false, &M, s, true))) return rc;
+        if ((rc = m2_dispatch<T>(h->phys, false, &M, s, true, h->tile))) return rc;
     } else {
         const T dt2 = (T)(h->dt * 0.5), dtt = (T)h->dt;
         // stage 1
         for (int f = 0; f < h->nf; ++f) A.out[f] = (T*)h->kbuf[0][f];
-        if ((rc = launch_stage<T>(h->phys, h->dim, MODE_K, A, s, h->tile))) return rc;
+        if ((rc = launch_stage3d<T>(h, MODE_K, A, s))) return rc;
         // stages 2, 3
         for (int st = 1; st < 3; ++st) {
             for (int f = 0; f < h->nf; ++f) {
@@ -813,7 +920,7 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s, int depth) {
                 A.out[f] = (T*)h->kbuf[st][f];
             }
             A.a = dt2;
-            if ((rc = launch_stage<T>(h->phys, h->dim, MODE_K, A, s, h->tile))) return rc;
+            if ((rc = launch_stage3d<T>(h, MODE_K, A, s))) return rc;
         }
         // stage 4 + update
         for (int f = 0; f < h->nf; ++f) {
@@ -825,7 +932,7 @@ static int enqueue_step(phix_stepper* h, cudaStream_t s, int depth) {
         A.a = dtt;
         A.dtf = (T)(h->dt / 6.0);
         set_lo(h->nf);
-        if ((rc = launch_stage<T>(h->phys, h->dim, MODE_RK4_FINAL, A, s, h->tile))) return rc;
+        if ((rc = launch_stage3d<T>(h, MODE_RK4_FINAL, A, s))) return rc;
     }
     h->cur = o;
     return PHIX_OK;
@@ -926,8 +1033,9 @@ int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precisio
     // measured on B200 at 1024^2: the one-launch step wins in FP32, and in FP64
     // where the pair kernel takes the grid (CH, four periodic sides); the
     // cell-per-thread step kernel loses to one launch per stage in FP64
-    h->fuse_steps = precision == PHIX_F32 || (phys == PHIX_PHYS_CH && step_pair_supported(L, g->dim)) ||
-                    (g->dim == 3 && phys != PHIX_PHYS_AC);
+    // 3-D: one launch per stage by default (measured faster on B200 than the
+    // fused two-stage launches, which the autotuner may still pick)
+    h->fuse_steps = g->dim < 3 && (precision == PHIX_F32 || (phys == PHIX_PHYS_CH && step_pair_supported(L, g->dim)));
     auto fail = [&](cudaError_t e, const char* w) {
         int r = cuda_status(e, w);
         phix_stepper_destroy(h);
@@ -961,6 +1069,14 @@ int phix_stepper_create(phix_stepper_t** out, int phys, int scheme, int precisio
     if ((rc = prepare_stage(phys, g->dim, precision))) {
         phix_stepper_destroy(h);
         return rc;
+    }
+    if (g->dim == 3 && scheme != PHIX_MULTISTEP && phys != PHIX_PHYS_AC) {
+        rc = precision == PHIX_F32 ? s3_dispatch<float>(phys, 0, true, nullptr, 0)
+                                   : s3_dispatch<double>(phys, 0, true, nullptr, 0);
+        if (rc) {
+            phix_stepper_destroy(h);
+            return rc;
+        }
     }
     if (g->dim == 3 && scheme == PHIX_RK4 && phys != PHIX_PHYS_AC) {
         rc = precision == PHIX_F32 ? m2_dispatch<float>(phys, true, nullptr, 0, false)
@@ -1057,7 +1173,11 @@ int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms) {
             for (int t = -1; t < kNumColCfgs; ++t) cand.push_back({false, t});
         else
             cand.push_back({false, -1});
-        if (h->dim == 3 && h->scheme == PHIX_RK4 && h->phys != PHIX_PHYS_AC) cand.push_back({true, -1});
+        if (h->dim == 3) cand.push_back({false, TILE3D_MARCH});  // the marching stage kernel
+        if (h->dim == 3 && h->scheme == PHIX_RK4 && h->phys != PHIX_PHYS_AC) {
+            cand.push_back({true, 0});  // the fused two-stage tile variants
+            cand.push_back({true, 1});
+        }
         if (h->scheme == PHIX_RK4 && h->nf == 1 && step2d_supported(h->L, h->dim))
             for (int t = 0; t < kNumStepCfgs + kNumPairCfgs; ++t) cand.push_back({true, t});
     }

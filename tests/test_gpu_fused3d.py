@@ -1,6 +1,7 @@
-"""The 3-D RK4 step in two launches of two fused stages (TMA plane staging,
-include/phix/detail/march3d_fused.cuh) against one launch per stage and the
-oracle, on a B200.
+"""The 3-D kernels with TMA plane staging on a B200: the RK4 step in two
+launches of two fused stages (include/phix/detail/march3d_fused.cuh) and the
+streamed one-stage kernel (include/phix/detail/stream3d.cuh, the default),
+against the marching stage kernel and the oracle.
 
 Grids are chosen to hit the kernel's edge cases: partial in-plane tiles, grids
 narrower than the four-cell halo, zero-flux and periodic in-plane sides, z
@@ -30,6 +31,7 @@ CASES = [
 PRM = {px.PHYS_CH: [1.0, 0.5, 1.0, 0.0, 1.0], px.PHYS_CHAC: [1.0, 1.0, 0.5, 0.5, 1.0]}
 DT = {px.PHYS_CH: 0.002, px.PHYS_CHAC: 0.002}
 NSTEPS = 9
+MARCH_TILE = 2  # phix_stepper_set_tiles on 3-D grids: the marching stage kernel (no TMA)
 
 
 def _inputs(phys, n, grid, seed):
@@ -41,9 +43,10 @@ def _inputs(phys, n, grid, seed):
     return f
 
 
-def _run(phys, g, prec, fields, fused, nsteps=NSTEPS, graph=0):
+def _run(phys, g, prec, fields, fused, nsteps=NSTEPS, graph=0, tile=-1):
     st = px.Stepper(phys, px.RK4, prec, PRM[phys], DT[phys], g)
     st.set_fusion(fused)
+    st.set_tiles(tile)
     lps = st.launches_per_step
     d = [torch.from_numpy(f.copy()).cuda() for f in fields]
     st.load(d)
@@ -66,12 +69,14 @@ def test_fused_3d_step_matches_per_stage_launches(cuda, oracle, prec, case):
     grid = Grid(n=n, bc=bcs)
     fields = _inputs(phys, n, grid, hash(n) % 1000)
     fused, lps_f = _run(phys, g, prec, fields, True)
-    staged, lps_s = _run(phys, g, prec, fields, False)
+    staged, lps_s = _run(phys, g, prec, fields, False)               # streamed TMA stage kernel
+    marched, _ = _run(phys, g, prec, fields, False, tile=MARCH_TILE)  # marching stage kernel
     assert lps_f == 2 and lps_s == 4  # odd FP64 rows too: the stepper's own arrays are row-padded
-    for a, b in zip(fused, staged):
-        pa, pb = grid.phys(a), grid.phys(b)
-        bad = np.argwhere(pa != pb)
-        assert bad.size == 0, f"{len(bad)} cells differ, first (z, y, x) {bad[:4].tolist()}"
+    for other in (fused, marched):
+        for a, b in zip(other, staged):
+            pa, pb = grid.phys(a), grid.phys(b)
+            bad = np.argwhere(pa != pb)
+            assert bad.size == 0, f"{len(bad)} cells differ, first (z, y, x) {bad[:4].tolist()}"
     if prec == px.F64:
         want = [f.copy() for f in fields]
         grid.fma_mode = 1
@@ -122,3 +127,53 @@ def test_fused_3d_on_bound_buffers_with_odd_rows_falls_back(cuda):
         ref, _ = _run(px.PHYS_CHAC, g, px.F64, fields, False, nsteps=4)
         for a, b in zip(got, ref):
             assert np.array_equal(grid.phys(a), grid.phys(b))
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32], ids=["f64", "f32"])
+@pytest.mark.parametrize("case", [CASES[0], CASES[2], CASES[3]], ids=lambda c: "x".join(map(str, c[1])))
+def test_fused_3d_tile_variants_agree(cuda, prec, case):
+    """Tile variant 1 (stages 3-4 on 32x8 tiles; FP64 also stages 1-2) gives
+    the bits of variant 0."""
+    phys, n, bx, by = case
+    bcs = (bx, bx, by, by, px.BC_PERIODIC, px.BC_PERIODIC)
+    g = px.make_grid(n, (1.0, 1.0, 1.0), 1, bcs)
+    grid = Grid(n=n, bc=bcs)
+    fields = _inputs(phys, n, grid, 17)
+    a, _ = _run(phys, g, prec, fields, True, tile=0)
+    b, lps = _run(phys, g, prec, fields, True, tile=1)
+    assert lps == 2
+    for x, y in zip(a, b):
+        assert np.array_equal(grid.phys(x), grid.phys(y))
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32], ids=["f64", "f32"])
+def test_streamed_3d_euler_and_graph_replay(cuda, oracle, prec):
+    """Euler steps and graph-replayed RK4 steps through the streamed stage
+    kernel give the marching kernel's bits (FP64: and the oracle's)."""
+    phys, n = px.PHYS_CHAC, (40, 24, 18)
+    bcs = (px.BC_NOFLUX, px.BC_NOFLUX) + (px.BC_PERIODIC,) * 4
+    g = px.make_grid(n, (1.0, 0.9, 1.1), 1, bcs)
+    grid = Grid(n=n, d=(1.0, 0.9, 1.1), bc=bcs)
+    fields = _inputs(phys, n, grid, 23)
+    for scheme, graph in ((px.EULER, 0), (px.RK4, 4)):
+        outs = []
+        for tile in (-1, MARCH_TILE):
+            st = px.Stepper(phys, scheme, prec, PRM[phys], DT[phys], g)
+            st.set_tiles(tile)
+            d = [torch.from_numpy(f.copy()).cuda() for f in fields]
+            st.load(d)
+            st.set_graph(graph)
+            st.advance(10)
+            st.store(d)
+            torch.cuda.synchronize()
+            st.status()
+            st.close()
+            outs.append([x.cpu().numpy() for x in d])
+        for a, b in zip(*outs):
+            assert np.array_equal(grid.phys(a), grid.phys(b)), scheme
+        if prec == px.F64:
+            want = [f.copy() for f in fields]
+            grid.fma_mode = 1
+            oracle.advance(want, phys, PRM[phys], scheme, DT[phys], 10, grid)
+            for a, b in zip(outs[0], want):
+                assert np.array_equal(grid.phys(a), grid.phys(b)), scheme

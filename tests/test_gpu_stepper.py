@@ -487,7 +487,7 @@ def test_temporal_blocking_depth2_matches_single_steps(cuda, oracle, prec, tile,
     rng = np.random.default_rng(7 + tile)
     x = grid.stored_from_phys(rng.uniform(0.3, 0.7, size=(1, n[1], n[0])))
     prm = [1.0, 0.6, 1.2, 0.05, 0.95]
-    outs = []
+    outs, launches = [], []
     for t in (tile, -1):
         st = px.Stepper(px.PHYS_CH, px.RK4, prec, prm, 0.004, g)
         st.set_tiles(t)
@@ -498,13 +498,13 @@ def test_temporal_blocking_depth2_matches_single_steps(cuda, oracle, prec, tile,
         before = px.launch_count()
         st.advance(nsteps)
         torch.cuda.synchronize()
-        launches = px.launch_count() - before
+        launches.append(px.launch_count() - before)
         st.store([d])
         torch.cuda.synchronize()
         st.close()
         outs.append(d.cpu().numpy())
-        if t == tile:
-            assert launches == nsteps // 2 + nsteps % 2
+    # the single-step run: the first step's BC fills plus one launch per step
+    assert launches[0] == launches[1] - nsteps + nsteps // 2 + nsteps % 2
     keep = ~corner_mask(grid)
     assert np.array_equal(outs[0][keep], outs[1][keep])
     if prec == px.F64:
