@@ -6,8 +6,10 @@
 // of its (TX + 4) x (TY + 4) threads owns one (x, y) column of the tile + 2.
 // Per input plane p:
 //   * the planes of u (and of the previous stage's k) arrive by TMA
-//     (cp.async.bulk.tensor.3d, one box per array and field) into a 3-slot ring,
-//     one mbarrier per slot, two planes ahead of their use;
+//     (cp.async.bulk.tensor.3d, one box per array and field) into a ring of
+//     slots, one mbarrier per slot, two (FP64) or three (FP32) planes ahead
+//     of their use; one thread waits for each copy, the others at the CTA
+//     barrier;
 //   * every thread forms its column's stage state y = u + a k_prev
 //     (kernel_rk4_tmp, Solver.cu:49-56), keeps it in a register window along z
 //     and writes it into a shared plane (in-plane neighbours only);
@@ -54,7 +56,9 @@ struct Stream3 {
     static constexpr int WB = (NX + VEC - 1 + VEC - 1) / VEC * VEC;  // box width = plane pitch (16-byte rows)
     static constexpr int HB = NY;
     static constexpr int PL = (WB * HB * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);  // 128-byte slots
-    static constexpr int NS = 3;  // input slots: plane p in use, p+1 and p+2 in flight
+    // input slots: planes p-2 .. p resident (the final stage reads u and the
+    // previous k of plane p-2 from them), LA planes in flight
+    static constexpr int LA = sizeof(T) == 4 ? 3 : 2, NS = 3 + LA;
     static constexpr int NY_R = 4, NM_R = 2;  // shared planes of y (p-3 .. p) and mu (p-2, p-1)
     static constexpr size_t OFF_IN = 0;                                        // [NS][2 arrays][NF][PL]
     static constexpr size_t OFF_Y = OFF_IN + (size_t)NS * 2 * NF * PL;          // [NY_R][NF][PL]
@@ -136,8 +140,9 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY>::NT)
         m2::fence_bar_init();
     }
     __syncthreads();
+    constexpr int LA = G::LA;
     if (threadIdx.x == 0)
-        for (int t = t_first; t < t_first + NS - 1 && t <= t_last; ++t) issue(t);
+        for (int t = t_first; t < t_first + LA && t <= t_last; ++t) issue(t);
 
     // register windows along z: c at p-2 .. p, eta at p-3 .. p, mu at p-3 .. p-1
     T w0[3], w1[4], wm[3];
@@ -147,11 +152,28 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY>::NT)
     for (int i = 0; i < 4; ++i) w1[i] = (T)0;
     const T a = S.a, i2x = S.i2[0], i2y = S.i2[1], i2z = S.i2[2];
     bool failed = false;
-    int issued = min(t_first + NS - 2, t_last);  // last plane whose copy was issued
+    int issued = min(t_first + LA - 1, t_last);  // last plane whose copy was issued
+    constexpr bool FINAL = MODE == MODE_RK4_FINAL || MODE == MODE_EULER_FINAL;
 
     for (int p = t_first; p <= t_last; ++p) {
-        // ---- the input plane p: wait, BC-map this column if it lies outside the grid
-        const bool ok = m2::bar_wait(bar(p), (uint32_t)(((p - t_first) / NS) & 1), m2::WAIT_NS);
+        // the final stage's k1, k2 and low parts of this thread's tile cell at
+        // plane p-2, fetched now so that they arrive while the plane is formed
+        T pk1[2] = {(T)0, (T)0}, pk2[2] = {(T)0, (T)0}, plo[2] = {(T)0, (T)0};
+        if (FINAL && in_tile && p - 2 >= z0 && p - 2 < z1) {
+            const int idx = L.origin + gtile + L.s[2] * (p - 2);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                if (MODE == MODE_RK4_FINAL) {
+                    pk1[f] = __ldg(S.k1[f] + idx);
+                    pk2[f] = __ldg(S.k2[f] + idx);
+                }
+                if (S.ulo[f]) plo[f] = __ldg(S.ulo[f] + idx);
+            }
+        }
+        // ---- the input plane p: one thread waits for its copy, the others at
+        //      the CTA barrier; then BC-map this column if it lies outside the grid
+        bool ok = true;
+        if (threadIdx.x == 0) ok = m2::bar_wait(bar(p), (uint32_t)(((p - t_first) / NS) & 1), m2::WAIT_NS);
         if (__syncthreads_or(!ok)) { failed = true; break; }
         T y[2];
         if (!ood) {
@@ -173,11 +195,11 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY>::NT)
 #pragma unroll
         for (int f = 0; f < NF; ++f) y_slot(f, p)[po] = y[f];
         __syncthreads();
-        // the slot of plane p is free: the copy of plane p + NS - 1 into it
-        if (threadIdx.x == 0 && p + NS - 1 <= t_last) {
+        // the slot of plane p-3 is free (last read by step p-1): plane p + LA into it
+        if (threadIdx.x == 0 && p + LA <= t_last) {
             m2::fence_proxy_async();
-            issue(p + NS - 1);
-            issued = p + NS - 1;
+            issue(p + LA);
+            issued = p + LA;
         }
         // ---- mu at plane p-1 on the tile + 1
         if (p - 1 >= z0 - 1 && p - 1 <= z1) {
@@ -218,7 +240,25 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY>::NT)
                 pol.rhs(S, lapmu, w0[0], (T)0, NF > 1 ? w1[1] : (T)0, lapy1, k);
                 const int idx = L.origin + gtile + L.s[2] * z;
 #pragma unroll
-                for (int f = 0; f < NF; ++f) emit<T, MODE>(S, f, idx, k[f]);
+                for (int f = 0; f < NF; ++f) {
+                    if constexpr (MODE == MODE_K) {
+                        S.out[f][idx] = k[f];
+                    } else {
+                        // emit's arithmetic, with u (and k3) from the plane's input slot
+                        const T u = in_slot(0, f, z)[po];
+                        T d;
+                        if constexpr (MODE == MODE_RK4_FINAL) {
+                            // phi += dt6 * (((k1 + 2 k2) + 2 k3) + k4)
+                            T sum = radd(pk1[f], rmul((T)2, pk2[f]));
+                            sum = radd(sum, rmul((T)2, in_slot(1, f, z)[po]));
+                            d = radd(sum, k[f]);
+                        } else {
+                            d = k[f];
+                        }
+                        if (S.ulo[f]) twosum_update(u, plo[f], rmul(S.dtf, d), &S.out[f][idx], &S.outlo[f][idx]);
+                        else S.out[f][idx] = rfma(S.dtf, d, u);
+                    }
+                }
             }
             if (MODE != MODE_K) {
                 // ghost cells of the new state (the BC-mapped old state), as stage_march3d writes them

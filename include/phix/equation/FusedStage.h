@@ -58,5 +58,26 @@ struct PolUser {
     }
 };
 
+// The two-term composite program of the Cahn-Hilliard form,
+// mu = c0 * f(y) + c1 * lap(y) (PW_FIRST) or c0 * lap(y) + c1 * f(y), with the
+// term order compiled in: the same multiply-adds as PolUser's walk over its
+// term list (acc = fma(c0, v0, 0); acc = fma(c1, v1, acc)), without the walk.
+template <class F, bool PW_FIRST>
+struct PolUserCH2 {
+    static constexpr int NF = 1, H = 2;
+    static constexpr bool MU = true, LAP_Y0 = false, LAP_Y1 = false;
+    F f;
+    double c0, c1, M;
+    template <typename T>
+    __device__ __forceinline__ T mu(const phix::StageArgs<T>&, T y, T lapy, T) const {
+        const double v0 = PW_FIRST ? (double)f(y) : lapy, v1 = PW_FIRST ? lapy : (double)f(y);
+        return __fma_rn(c1, v1, __fma_rn(c0, v0, 0.0));
+    }
+    template <typename T>
+    __device__ __forceinline__ void rhs(const phix::StageArgs<T>&, T lapmu, T, T, T, T, T* k) const {
+        k[0] = __fma_rn(M, lapmu, 0.0);
+    }
+};
+
 }  // namespace fuse
 }  // namespace PhiX

@@ -79,7 +79,20 @@ struct PwKernelsImpl final : fuse::PwKernels {
                 B.dt2 = s.dt_half;
                 B.dt = s.dt_full;
                 dim3 grid((A.L.n[0] + 63) / 64, (A.L.n[1] + 27) / 28, 1);
-                phix::step_pair<double, Pol, 64, 28, 8><<<grid, G::NT, G::smem_bytes(), st>>>(B, pol);
+                if (s.nops == 2 && s.op[0] != s.op[1]) {
+                    // the two-term CH program (pw and lap, either order) compiled in
+                    if (s.op[0] == fuse::OP_PW) {
+                        fuse::PolUserCH2<F, true> p2{func, s.c[0], s.c[1], s.M};
+                        phix::step_pair<double, fuse::PolUserCH2<F, true>, 64, 28, 8>
+                            <<<grid, G::NT, G::smem_bytes(), st>>>(B, p2);
+                    } else {
+                        fuse::PolUserCH2<F, false> p2{func, s.c[0], s.c[1], s.M};
+                        phix::step_pair<double, fuse::PolUserCH2<F, false>, 64, 28, 8>
+                            <<<grid, G::NT, G::smem_bytes(), st>>>(B, p2);
+                    }
+                } else {
+                    phix::step_pair<double, Pol, 64, 28, 8><<<grid, G::NT, G::smem_bytes(), st>>>(B, pol);
+                }
                 count_user_launch();
                 return cudaGetLastError() == cudaSuccess ? PHIX_OK : PHIX_ERR_CUDA;
             } else {
@@ -153,8 +166,15 @@ struct PwKernelsImpl final : fuse::PwKernels {
         if (dim == 2) {  // the one-launch RK4 step's shared memory (99 KB)
             using Pol = fuse::PolUser<F, fuse::PATTERN_COMPOSITE>;
             using G = phix::StepPair<double, 64, 28, 8>;
+            const int b = (int)G::smem_bytes();
             cudaError_t e = cudaFuncSetAttribute(phix::step_pair<double, Pol, 64, 28, 8>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes());
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(phix::step_pair<double, fuse::PolUserCH2<F, true>, 64, 28, 8>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(phix::step_pair<double, fuse::PolUserCH2<F, false>, 64, 28, 8>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, b);
             return e == cudaSuccess ? PHIX_OK : PHIX_ERR_CUDA;
         }
         if (dim != 3) return PHIX_OK;

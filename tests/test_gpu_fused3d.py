@@ -115,6 +115,7 @@ def test_fused_3d_on_bound_buffers_with_odd_rows_falls_back(cuda):
         grid = Grid(n=n, bc=bcs)
         fields = _inputs(px.PHYS_CHAC, n, grid, 3)
         st = px.Stepper(px.PHYS_CHAC, px.RK4, px.F64, PRM[px.PHYS_CHAC], DT[px.PHYS_CHAC], g)
+        st.set_fusion(True)  # the fused two-stage launches (one launch per stage is the 3-D default)
         d = [torch.from_numpy(f.copy()).cuda() for f in fields]
         alt = [x.clone() for x in d]
         st.bind(d, alt)

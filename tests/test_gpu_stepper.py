@@ -503,8 +503,12 @@ def test_temporal_blocking_depth2_matches_single_steps(cuda, oracle, prec, tile,
         torch.cuda.synchronize()
         st.close()
         outs.append(d.cpu().numpy())
-    # the single-step run: the first step's BC fills plus one launch per step
-    assert launches[0] == launches[1] - nsteps + nsteps // 2 + nsteps % 2
+    # the single-step run: the first step's BC fills plus one launch per step;
+    # depth 2 pairs the steps of each graph group (an odd group or remainder
+    # ends with a single-step launch)
+    pairs = lambda k: k // 2 + k % 2
+    want = pairs(nsteps) if not graph else (nsteps // graph) * pairs(graph) + pairs(nsteps % graph)
+    assert launches[0] == launches[1] - nsteps + want
     keep = ~corner_mask(grid)
     assert np.array_equal(outs[0][keep], outs[1][keep])
     if prec == px.F64:

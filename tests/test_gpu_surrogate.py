@@ -1,7 +1,7 @@
 """Tensor-core surrogate kernels (tcgen05 implicit-GEMM convolutions) against
 the numpy oracle: forward output, all eight gradient tensors, and the exact
-FP64 mean-mass projection.  Tolerances reflect BF16 activations and FP32
-accumulation (the oracle accumulates in FP64)."""
+FP64 mean-mass projection.  Tolerances are three times the errors measured on
+a B200 (BF16 activations and FP32 accumulation against the oracle's FP64)."""
 import numpy as np
 import pytest
 import torch
@@ -42,7 +42,7 @@ def test_forward_matches_oracle(cuda):
     want, _ = so.forward(params, c, SHIFT, SCALE)
     got = o.cpu().numpy()
     print("forward rel-L2", rel(got, want))
-    assert rel(got, want) < 1e-2
+    assert rel(got, want) < 3.2e-3  # three times the 1.04e-3 measured on a B200
     sg.close()
 
 
@@ -58,7 +58,7 @@ def test_gradients_match_oracle(cuda):
     for name, a, b in zip(["W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4"], got, want):
         r = rel(a.reshape(b.shape), b)
         print(f"{name}: rel-L2 {r:.3e}")
-        assert r < 5e-2, name
+        assert r < 1.6e-3, name  # three times the largest measured on a B200 (W1: 5.4e-4)
     sg.close()
 
 
