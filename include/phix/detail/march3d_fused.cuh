@@ -87,6 +87,28 @@ __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, uint64_t 
     return true;
 }
 
+// The same wait with the waiting thread suspended inside each try (up to
+// 20 us, woken early when the phase completes) instead of spinning, so that
+// it takes no issue slots from the CTA's other warps.
+__device__ __forceinline__ bool bar_try_wait_sleep(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity), "r"(20000u)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool bar_wait_sleep(uint64_t* b, uint32_t parity, uint64_t limit_ns) {
+    if (bar_try_wait_sleep(b, parity)) return true;
+    const uint64_t t0 = now_ns();
+    while (!bar_try_wait_sleep(b, parity))
+        if (now_ns() - t0 > limit_ns) return false;
+    return true;
+}
+
 constexpr uint64_t WAIT_NS = 2000000000ull;  // a plane copy that takes 2 s has failed
 
 }  // namespace m2

@@ -48,7 +48,7 @@ struct Stream3Args {
     int* err;           // set when a plane copy did not arrive in time
 };
 
-template <typename T, class Pol, int TX, int TY>
+template <typename T, class Pol, int TX, int TY, bool FINAL>
 struct Stream3 {
     static constexpr int NF = Pol::NF, H = Pol::H;
     static constexpr int NX = TX + 2 * H, NY = TY + 2 * H, NT = NX * NY;  // one thread per column of the tile + 2
@@ -56,9 +56,11 @@ struct Stream3 {
     static constexpr int WB = (NX + VEC - 1 + VEC - 1) / VEC * VEC;  // box width = plane pitch (16-byte rows)
     static constexpr int HB = NY;
     static constexpr int PL = (WB * HB * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);  // 128-byte slots
-    // input slots: planes p-2 .. p resident (the final stage reads u and the
-    // previous k of plane p-2 from them), LA planes in flight
-    static constexpr int LA = sizeof(T) == 4 ? 3 : 2, NS = 3 + LA;
+    // input slots: LA planes in flight beyond the plane in use; the final
+    // stage keeps planes p-2 .. p resident (it reads u and the previous k of
+    // plane p-2 from them), the others only plane p
+    static constexpr int RES = FINAL ? 3 : 1;
+    static constexpr int LA = FINAL ? (sizeof(T) == 4 ? 3 : 2) : (sizeof(T) == 4 ? 6 : 4), NS = RES + LA;
     static constexpr int NY_R = 4, NM_R = 2;  // shared planes of y (p-3 .. p) and mu (p-2, p-1)
     static constexpr size_t OFF_IN = 0;                                        // [NS][2 arrays][NF][PL]
     static constexpr size_t OFF_Y = OFF_IN + (size_t)NS * 2 * NF * PL;          // [NY_R][NF][PL]
@@ -72,9 +74,9 @@ struct Stream3 {
 };
 
 template <typename T, class Pol, int MODE, int TX, int TY>
-__global__ void __launch_bounds__(Stream3<T, Pol, TX, TY>::NT)
+__global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, MODE != MODE_K>::NT)
     stage_stream3d(const __grid_constant__ Stream3Args<T> A) {
-    using G = Stream3<T, Pol, TX, TY>;
+    using G = Stream3<T, Pol, TX, TY, MODE != MODE_K>;
     constexpr int NF = G::NF, H = G::H, NX = G::NX, WB = G::WB, PL = G::PL, NS = G::NS;
     constexpr int NYR = G::NY_R, NMR = G::NM_R;
     const Pol pol{};
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY>::NT)
         // ---- the input plane p: one thread waits for its copy, the others at
         //      the CTA barrier; then BC-map this column if it lies outside the grid
         bool ok = true;
-        if (threadIdx.x == 0) ok = m2::bar_wait(bar(p), (uint32_t)(((p - t_first) / NS) & 1), m2::WAIT_NS);
+        if (threadIdx.x == 0) ok = m2::bar_wait_sleep(bar(p), (uint32_t)(((p - t_first) / NS) & 1), m2::WAIT_NS);
         if (__syncthreads_or(!ok)) { failed = true; break; }
         T y[2];
         if (!ood) {
@@ -195,7 +197,7 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY>::NT)
 #pragma unroll
         for (int f = 0; f < NF; ++f) y_slot(f, p)[po] = y[f];
         __syncthreads();
-        // the slot of plane p-3 is free (last read by step p-1): plane p + LA into it
+        // the slot of plane p - RES is free (last read by step p-1): plane p + LA into it
         if (threadIdx.x == 0 && p + LA <= t_last) {
             m2::fence_proxy_async();
             issue(p + LA);

@@ -734,7 +734,7 @@ template <> struct S3Cfg<double> { static constexpr int TX = 32, TY = 8; };
 template <typename T, class Pol, int MODE>
 int s3_kernel(bool prepare, Stream3Args<T>* a, cudaStream_t s) {
     using C = S3Cfg<T>;
-    using G = Stream3<T, Pol, C::TX, C::TY>;
+    using G = Stream3<T, Pol, C::TX, C::TY, MODE != MODE_K>;
     auto kern = stage_stream3d<T, Pol, MODE, C::TX, C::TY>;
     if (prepare) {
         PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
