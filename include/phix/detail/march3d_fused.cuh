@@ -167,8 +167,10 @@ __global__ void __launch_bounds__(NT) stage2_march3d(const __grid_constant__ Mar
     const Pol pol{};
     const StageArgs<T>& S = A.S;
     const Layout& L = S.L;
-    extern __shared__ unsigned char m2_raw[];
-    T* sm = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(m2_raw) + 127) & ~(uintptr_t)127);
+    // 128-byte aligned slots, offset from the shared array itself so that slot
+    // accesses stay shared-memory accesses
+    extern __shared__ __align__(128) unsigned char m2_raw[];
+    T* sm = reinterpret_cast<T*>(m2_raw + ((128u - (m2::saddr(m2_raw) & 127u)) & 127u));
     uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(sm) + G::BAR_OFF);  // NU mbarriers
 
     const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2], gh = L.ghost;
@@ -206,7 +208,11 @@ __global__ void __launch_bounds__(NT) stage2_march3d(const __grid_constant__ Mar
         }
         return soff(lx, ly);
     };
-    auto zwrap = [&](int z) { const int r = z % n2; return r < 0 ? r + n2 : r; };
+    auto zwrap = [&](int z) {
+        if ((unsigned)z < (unsigned)n2) return z;
+        const int r = z % n2;
+        return r < 0 ? r + n2 : r;
+    };
 
     // input planes z0 - E .. z1 + E - 1 (each stage reaches H = 2 planes)
     const int t_first = z0 - E, t_last = z1 + E - 1;

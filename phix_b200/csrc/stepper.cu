@@ -726,16 +726,23 @@ int m2_dispatch(int phys, bool prepare, March2Args<T>* a, cudaStream_t s, bool s
 }
 
 // ---- one stage of the mu physics streamed through z (stream3d.cuh) --------
-// tile per precision: TX x TY, (TX + 4) x (TY + 4) threads
-template <typename T> struct S3Cfg;
-template <> struct S3Cfg<float> { static constexpr int TX = 32, TY = 8; };
-template <> struct S3Cfg<double> { static constexpr int TX = 32, TY = 8; };
+// tile variants per precision: TX x TY tile, R rows of a column per thread,
+// (TX + 4) x (TY + 4) / R threads
+constexpr int kNumS3Variants = 3;
+template <typename T, int V> struct S3Cfg;
+template <> struct S3Cfg<float, 0> { static constexpr int TX = 32, TY = 8, R = 1; };
+template <> struct S3Cfg<float, 1> { static constexpr int TX = 32, TY = 16, R = 4; };
+template <> struct S3Cfg<float, 2> { static constexpr int TX = 32, TY = 8, R = 2; };
+template <> struct S3Cfg<double, 0> { static constexpr int TX = 32, TY = 8, R = 1; };
+template <> struct S3Cfg<double, 1> { static constexpr int TX = 32, TY = 8, R = 2; };
+template <> struct S3Cfg<double, 2> { static constexpr int TX = 32, TY = 8, R = 4; };
 
-template <typename T, class Pol, int MODE>
+template <typename T, class Pol, int MODE, int V>
 int s3_kernel(bool prepare, Stream3Args<T>* a, cudaStream_t s) {
-    using C = S3Cfg<T>;
-    using G = Stream3<T, Pol, C::TX, C::TY, MODE != MODE_K>;
-    auto kern = stage_stream3d<T, Pol, MODE, C::TX, C::TY>;
+    using C = S3Cfg<T, V>;
+    using G = Stream3<T, Pol, C::TX, C::TY, C::R, MODE != MODE_K>;
+    static_assert(G::smem_bytes() <= 227 * 1024, "streamed 3-D tile too large");
+    auto kern = stage_stream3d<T, Pol, MODE, C::TX, C::TY, C::R>;
     if (prepare) {
         PHIX_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()));
         return PHIX_OK;
@@ -762,26 +769,43 @@ int s3_kernel(bool prepare, Stream3Args<T>* a, cudaStream_t s) {
     return PHIX_OK;
 }
 
-template <typename T, class Pol>
-int s3_mode(int mode, bool prepare, Stream3Args<T>* a, cudaStream_t s) {
+template <typename T, class Pol, int V>
+int s3_mode_v(int mode, bool prepare, Stream3Args<T>* a, cudaStream_t s) {
     if (prepare) {
-        int rc = s3_kernel<T, Pol, MODE_K>(true, a, s);
-        if (!rc) rc = s3_kernel<T, Pol, MODE_RK4_FINAL>(true, a, s);
-        return rc ? rc : s3_kernel<T, Pol, MODE_EULER_FINAL>(true, a, s);
+        int rc = s3_kernel<T, Pol, MODE_K, V>(true, a, s);
+        if (!rc) rc = s3_kernel<T, Pol, MODE_RK4_FINAL, V>(true, a, s);
+        return rc ? rc : s3_kernel<T, Pol, MODE_EULER_FINAL, V>(true, a, s);
     }
     switch (mode) {
-        case MODE_K: return s3_kernel<T, Pol, MODE_K>(false, a, s);
-        case MODE_RK4_FINAL: return s3_kernel<T, Pol, MODE_RK4_FINAL>(false, a, s);
-        case MODE_EULER_FINAL: return s3_kernel<T, Pol, MODE_EULER_FINAL>(false, a, s);
+        case MODE_K: return s3_kernel<T, Pol, MODE_K, V>(false, a, s);
+        case MODE_RK4_FINAL: return s3_kernel<T, Pol, MODE_RK4_FINAL, V>(false, a, s);
+        case MODE_EULER_FINAL: return s3_kernel<T, Pol, MODE_EULER_FINAL, V>(false, a, s);
     }
     set_error("stage_stream3d: mode %d", mode);
     return PHIX_ERR_UNSUPPORTED;
 }
 
+// prepare: every variant; else the one asked for
+template <typename T, class Pol>
+int s3_mode(int mode, bool prepare, Stream3Args<T>* a, cudaStream_t s, int variant) {
+    if (prepare) {
+        int rc = s3_mode_v<T, Pol, 0>(mode, true, a, s);
+        if (!rc) rc = s3_mode_v<T, Pol, 1>(mode, true, a, s);
+        return rc ? rc : s3_mode_v<T, Pol, 2>(mode, true, a, s);
+    }
+    switch (variant) {
+        case 0: return s3_mode_v<T, Pol, 0>(mode, false, a, s);
+        case 1: return s3_mode_v<T, Pol, 1>(mode, false, a, s);
+        case 2: return s3_mode_v<T, Pol, 2>(mode, false, a, s);
+    }
+    set_error("stage_stream3d: tile variant %d (0..%d)", variant, kNumS3Variants - 1);
+    return PHIX_ERR_UNSUPPORTED;
+}
+
 template <typename T>
-int s3_dispatch(int phys, int mode, bool prepare, Stream3Args<T>* a, cudaStream_t s) {
-    if (phys == PHIX_PHYS_CH) return s3_mode<T, PolCH>(mode, prepare, a, s);
-    if (phys == PHIX_PHYS_CHAC) return s3_mode<T, PolCHAC>(mode, prepare, a, s);
+int s3_dispatch(int phys, int mode, bool prepare, Stream3Args<T>* a, cudaStream_t s, int variant = 0) {
+    if (phys == PHIX_PHYS_CH) return s3_mode<T, PolCH>(mode, prepare, a, s, variant);
+    if (phys == PHIX_PHYS_CHAC) return s3_mode<T, PolCHAC>(mode, prepare, a, s, variant);
     set_error("stage_stream3d: physics %d has no chemical potential", phys);
     return PHIX_ERR_UNSUPPORTED;
 }
@@ -807,6 +831,9 @@ static bool tma3d_ok(const phix_stepper* h) {
 // Tile configuration of 3-D steppers that selects the marching stage kernel
 // (no TMA) for one launch per stage.
 constexpr int TILE3D_MARCH = 2;
+// Tile configurations 3 .. 3 + kNumS3Variants - 1 of 3-D steppers: the
+// streamed stage kernel's tile variants (-1, 0 and 1: variant 0).
+constexpr int TILE3D_STREAM = 3;
 
 // One 3-D stage: streamed with TMA staging where tma3d_ok (unless the tile
 // configuration asks for the marching kernel), else stage_march3d.
@@ -817,7 +844,8 @@ static int launch_stage3d(const phix_stepper* h, int mode, const StageArgs<T>& A
         memset(&a, 0, sizeof(a));
         a.S = A;
         a.err = h->err;
-        return s3_dispatch<T>(h->phys, mode, false, &a, s);
+        const int v = h->tile >= TILE3D_STREAM && h->tile < TILE3D_STREAM + kNumS3Variants ? h->tile - TILE3D_STREAM : 0;
+        return s3_dispatch<T>(h->phys, mode, false, &a, s, v);
     }
     return launch_stage<T>(h->phys, h->dim, mode, A, s, h->tile);
 }
@@ -1173,7 +1201,10 @@ int phix_stepper_autotune(phix_stepper_t* h, int trial_steps, double* best_ms) {
             for (int t = -1; t < kNumColCfgs; ++t) cand.push_back({false, t});
         else
             cand.push_back({false, -1});
-        if (h->dim == 3) cand.push_back({false, TILE3D_MARCH});  // the marching stage kernel
+        if (h->dim == 3) {
+            cand.push_back({false, TILE3D_MARCH});  // the marching stage kernel
+            for (int v = 1; v < kNumS3Variants; ++v) cand.push_back({false, TILE3D_STREAM + v});  // streamed variants
+        }
         if (h->dim == 3 && h->scheme == PHIX_RK4 && h->phys != PHIX_PHYS_AC) {
             cand.push_back({true, 0});  // the fused two-stage tile variants
             cand.push_back({true, 1});

@@ -32,6 +32,7 @@ PRM = {px.PHYS_CH: [1.0, 0.5, 1.0, 0.0, 1.0], px.PHYS_CHAC: [1.0, 1.0, 0.5, 0.5,
 DT = {px.PHYS_CH: 0.002, px.PHYS_CHAC: 0.002}
 NSTEPS = 9
 MARCH_TILE = 2  # phix_stepper_set_tiles on 3-D grids: the marching stage kernel (no TMA)
+STREAM_TILES = (3, 4, 5)  # the streamed stage kernel's tile variants (-1 = variant 0)
 
 
 def _inputs(phys, n, grid, seed):
@@ -178,3 +179,23 @@ def test_streamed_3d_euler_and_graph_replay(cuda, oracle, prec):
             oracle.advance(want, phys, PRM[phys], scheme, DT[phys], 10, grid)
             for a, b in zip(outs[0], want):
                 assert np.array_equal(grid.phys(a), grid.phys(b)), scheme
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32], ids=["f64", "f32"])
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "x".join(map(str, c[1])))
+def test_streamed_3d_tile_variants_agree(cuda, prec, case):
+    """Every tile variant of the streamed stage kernel (TX x TY tiles, R rows
+    of a column per thread) gives the marching kernel's bits."""
+    phys, n, bx, by = case
+    bcs = (bx, bx, by, by, px.BC_PERIODIC, px.BC_PERIODIC)
+    g = px.make_grid(n, (1.0, 1.0, 1.0), 1, bcs)
+    grid = Grid(n=n, bc=bcs)
+    fields = _inputs(phys, n, grid, 29)
+    ref, _ = _run(phys, g, prec, fields, False, nsteps=5, tile=MARCH_TILE)
+    for tile in STREAM_TILES:
+        got, lps = _run(phys, g, prec, fields, False, nsteps=5, tile=tile)
+        assert lps == 4
+        for a, b in zip(got, ref):
+            pa, pb = grid.phys(a), grid.phys(b)
+            bad = np.argwhere(pa != pb)
+            assert bad.size == 0, f"tile {tile}: {len(bad)} cells differ, first (z, y, x) {bad[:4].tolist()}"
