@@ -62,6 +62,13 @@ __device__ __forceinline__ void tma_box3(void* dst, const CUtensorMap* map, int 
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(saddr(b))
         : "memory");
 }
+// Prefetch one box of a 3-D tensor map into L2 (no shared memory, no completion).
+__device__ __forceinline__ void tma_prefetch3(const CUtensorMap* map, int x, int y, int z) {
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
 __device__ __forceinline__ bool bar_try_wait(uint64_t* b, uint32_t parity) {
     uint32_t ok;
     asm volatile(

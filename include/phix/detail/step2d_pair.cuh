@@ -450,6 +450,12 @@ template <typename T, class Pol, int TX, int TY, int NRP, int NS = 1>
 __global__ void __launch_bounds__(StepPair<T, TX, TY, NRP, NS>::NT, StepPair<T, TX, TY, NRP, NS>::MINB)
     step_pair(const StepArgs<T> A, const Pol pol) {
     extern __shared__ __align__(16) unsigned char step_smem[];
+    // launched as a programmatic dependent of the previous step (the C++
+    // Solver's launches): let the next step's CTAs be scheduled once every CTA
+    // of this one runs, and read nothing before the previous step's writes are
+    // visible.  Both are no-ops for an ordinary launch.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     step_pair_tile<T, Pol, TX, TY, NRP, NS>(A, pol, reinterpret_cast<T*>(step_smem), blockIdx.x * TX,
                                             blockIdx.y * TY);
 }

@@ -45,6 +45,12 @@ struct Stream3Args {
     StageArgs<T> S;
     CUtensorMap tu[2];  // u of each field
     CUtensorMap tk[2];  // the previous stage's k of each field (when S.kin is set)
+    // final stages: k1, k2 and the low parts of each field, boxes of the tile
+    // rows (TX + 16 bytes wide) that FP64 updates prefetch into L2 LA planes
+    // ahead of their loads (FP32 updates measured faster without); bit 2 j + f
+    // of pfm marks tq[j][f] as encoded
+    CUtensorMap tq[3][2];
+    int pfm;
     int rz;             // output planes per CTA
     int* err;           // set when a plane copy did not arrive in time
 };
@@ -263,6 +269,18 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, R, MODE != MODE_K>::NT
             m2::fence_proxy_async();
             issue(p + LA, si + LA < NS ? si + LA : si + LA - NS);
             issued = p + LA;
+        }
+        if (FINAL && sizeof(T) == 8 && threadIdx.x == 0 && A.pfm) {
+            // k1, k2 and the low parts of the plane updated LA steps from now
+            const int zp = p + LA - 2;
+            if (zp >= z0 && zp < z1) {
+                const int xq = x0 + gh - gh % G::VEC;
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int f = 0; f < NF; ++f)
+                        if ((A.pfm >> (2 * j + f)) & 1) m2::tma_prefetch3(&A.tq[j][f], xq, y0 + gh, zp + gh);
+            }
         }
         // ---- mu at plane p-1 on the tile + 1.  Every row of the thread is
         //      formed (rows off the tile + 1 read in-bounds values nobody uses and

@@ -79,22 +79,42 @@ struct PwKernelsImpl final : fuse::PwKernels {
                 B.dt2 = s.dt_half;
                 B.dt = s.dt_full;
                 dim3 grid((A.L.n[0] + 63) / 64, (A.L.n[1] + 27) / 28, 1);
-                if (s.nops == 2 && s.op[0] != s.op[1]) {
-                    // the two-term CH program (pw and lap, either order) compiled in
-                    if (s.op[0] == fuse::OP_PW) {
-                        fuse::PolUserCH2<F, true> p2{func, s.c[0], s.c[1], s.M};
-                        phix::step_pair<double, fuse::PolUserCH2<F, true>, 64, 28, 8>
-                            <<<grid, G::NT, G::smem_bytes(), st>>>(B, p2);
-                    } else {
+                // one launch per Solver::advance: each step is a programmatic
+                // dependent of the previous one, so its CTAs are resident and
+                // waiting (griddepcontrol.wait in step_pair) when that one ends
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = grid;
+                cfg.blockDim = dim3(G::NT);
+                cfg.dynamicSmemBytes = G::smem_bytes();
+                cfg.stream = st;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                at[0].val.programmaticStreamSerializationAllowed = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                auto go = [&]() -> cudaError_t {
+                    if (s.nops == 2 && s.op[0] != s.op[1]) {
+                        // the two-term CH program (pw and lap, either order) compiled in
+                        if (s.op[0] == fuse::OP_PW) {
+                            fuse::PolUserCH2<F, true> p2{func, s.c[0], s.c[1], s.M};
+                            return cudaLaunchKernelEx(&cfg, phix::step_pair<double, fuse::PolUserCH2<F, true>, 64, 28, 8>,
+                                                      B, p2);
+                        }
                         fuse::PolUserCH2<F, false> p2{func, s.c[0], s.c[1], s.M};
-                        phix::step_pair<double, fuse::PolUserCH2<F, false>, 64, 28, 8>
-                            <<<grid, G::NT, G::smem_bytes(), st>>>(B, p2);
+                        return cudaLaunchKernelEx(&cfg, phix::step_pair<double, fuse::PolUserCH2<F, false>, 64, 28, 8>,
+                                                  B, p2);
                     }
-                } else {
-                    phix::step_pair<double, Pol, 64, 28, 8><<<grid, G::NT, G::smem_bytes(), st>>>(B, pol);
+                    return cudaLaunchKernelEx(&cfg, phix::step_pair<double, Pol, 64, 28, 8>, B, pol);
+                };
+                cudaError_t e = go();
+                if (e == cudaErrorNotSupported || e == cudaErrorInvalidValue) {
+                    // a stream or device without dependent launches: an ordinary launch
+                    (void)cudaGetLastError();
+                    cfg.numAttrs = 0;
+                    e = go();
                 }
                 count_user_launch();
-                return cudaGetLastError() == cudaSuccess ? PHIX_OK : PHIX_ERR_CUDA;
+                return e == cudaSuccess && cudaGetLastError() == cudaSuccess ? PHIX_OK : PHIX_ERR_CUDA;
             } else {
                 return PHIX_ERR_UNSUPPORTED;
             }

@@ -237,7 +237,30 @@ int pair_cfg(bool prepare, const StepArgs<T>* A, cudaStream_t s, int* occ = null
         return PHIX_OK;
     }
     dim3 grid((A->S.L.n[0] + TX - 1) / TX, (A->S.L.n[1] + TY - 1) / TY, 1);
-    step_pair<T, PolCH, TX, TY, NRP, NS><<<grid, G::NT, G::smem_bytes(), s>>>(*A, PolCH{});
+    // launched one by one (not into a graph), each step is a programmatic
+    // dependent of the previous launch on the stream: its CTAs are scheduled
+    // while the previous step's last wave runs and wait in the kernel
+    // (griddepcontrol.wait) for that step's writes.  Graph replays keep plain
+    // edges: dependent launches measured 1-3 % slower there.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PHIX_TRY_CUDA(cudaStreamIsCapturing(s, &cap));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(G::NT);
+    cfg.dynamicSmemBytes = G::smem_bytes();
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = cap == cudaStreamCaptureStatusNone ? 1 : 0;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, step_pair<T, PolCH, TX, TY, NRP, NS>, *A, PolCH{});
+    if (e == cudaErrorNotSupported || e == cudaErrorInvalidValue) {
+        (void)cudaGetLastError();  // a stream without dependent launches: an ordinary launch
+        cfg.numAttrs = 0;
+        e = cudaLaunchKernelEx(&cfg, step_pair<T, PolCH, TX, TY, NRP, NS>, *A, PolCH{});
+    }
+    if (e != cudaSuccess) return cuda_status(e, "step_pair launch");
     PHIX_LAUNCH_CHECK("step_pair");
     return PHIX_OK;
 }
@@ -760,6 +783,19 @@ int s3_kernel(bool prepare, Stream3Args<T>* a, cudaStream_t s) {
     for (int f = 0; f < G::NF; ++f) {
         if ((rc = plane_map(&a->tu[f], a->S.u[f], L, (int)sizeof(T), G::WB, G::HB))) return rc;
         if (a->S.kin[0] && (rc = plane_map(&a->tk[f], a->S.kin[f], L, (int)sizeof(T), G::WB, G::HB))) return rc;
+    }
+    a->pfm = 0;
+    if (MODE != MODE_K && sizeof(T) == 8) {
+        // L2 prefetch boxes of the update's other operands (16-byte aligned arrays only)
+        for (int f = 0; f < G::NF; ++f) {
+            const void* src[3] = {MODE == MODE_RK4_FINAL ? a->S.k1[f] : nullptr,
+                                  MODE == MODE_RK4_FINAL ? a->S.k2[f] : nullptr, a->S.ulo[f]};
+            for (int j = 0; j < 3; ++j) {
+                if (!src[j] || (uintptr_t)src[j] % 16 != 0) continue;
+                if ((rc = plane_map(&a->tq[j][f], src[j], L, (int)sizeof(T), C::TX + G::VEC, C::TY))) return rc;
+                a->pfm |= 1 << (2 * j + f);
+            }
+        }
     }
     const long long cols = (long long)((L.n[0] + C::TX - 1) / C::TX) * ((L.n[1] + C::TY - 1) / C::TY);
     a->rz = pick_rz(cols, L.n[2], slots, G::H);
