@@ -35,6 +35,8 @@
 #include <cuda.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "phix/detail/march3d_fused.cuh"
 #include "phix/detail/stage.cuh"
 
@@ -173,38 +175,55 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, R, MODE != MODE_K>::NT
     if (threadIdx.x == 0)
         for (int t = t_first; t < t_first + LA && t <= t_last; ++t) issue(t, t - t_first);
 
-    // register windows along z, per row: c at p-2 .. p, eta at p-3 .. p, mu at p-3 .. p-1
-    T w0[R][3], w1[R][4], wm[R][3];
+    // register windows along z, per row, as rings over the plane's position
+    // J = (p - t_first) mod 4, which the march below makes a compile-time
+    // index: c of planes p-2 .. p, eta of p-3 .. p, mu of p-3 .. p-1
+    T w0[R][4], w1[R][4], wm[R][4];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
+    for (int r = 0; r < R; ++r)
 #pragma unroll
-        for (int i = 0; i < 3; ++i) w0[r][i] = wm[r][i] = (T)0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) w1[r][i] = (T)0;
-    }
+        for (int i = 0; i < 4; ++i) w0[r][i] = w1[r][i] = wm[r][i] = (T)0;
     const T a = S.a, i2x = S.i2[0], i2y = S.i2[1], i2z = S.i2[2];
     bool failed = false;
     int issued = min(t_first + LA - 1, t_last);  // last plane whose copy was issued
-    int si = 0, yi = 0;                          // input and y slots of plane p
-    uint32_t ph = 0;                             // phase parity of the input slot's mbarrier
+    int si = 0;        // input slot of plane p
+    uint32_t ph = 0;   // phase parity of the input slot's mbarrier
 
-    for (int p = t_first; p <= t_last; ++p) {
-        const int q = p - t_first;
+    // One input plane p.  Jc = 0..3: the plane's ring position (p - t_first)
+    // mod 4, compile-time, which indexes the y and mu slots and the register
+    // windows; Jc = -1: a rolling loop, the windows shifted by one plane and the
+    // slots indexed at run time (the update's form: unrolled, its extra
+    // operands exceed the register budget).  DO_MU: mu of plane p-1 is formed,
+    // DO_K: the right-hand side of plane p-2.  False: a copy did not arrive.
+    auto plane = [&](auto Jc, auto MUc, auto Kc, const int p) -> bool {
+        constexpr bool SHIFT = decltype(Jc)::value < 0;
+        constexpr int J = SHIFT ? 3 : decltype(Jc)::value;                   // window index of plane p
+        constexpr int J1 = (J + 3) & 3, J2 = (J + 2) & 3, J3 = (J + 1) & 3;  // planes p-1, p-2, p-3
+        constexpr bool DO_MU = decltype(MUc)::value, DO_K = decltype(Kc)::value;
+        const int jy = SHIFT ? ((p - t_first) & 3) : J;  // y slot of plane p
         T* const in_p = in_base(si);
         T* const in_p2 = in_base(si >= 2 ? si - 2 : si + NS - 2);  // plane p-2 (final stage)
-        T* const y_p = sm + G::OFF_Y + (size_t)yi * NF * PL;
-        T* const y_p1 = sm + G::OFF_Y + (size_t)((yi + 3) & 3) * NF * PL;
-        T* const y_p2 = sm + G::OFF_Y + (size_t)((yi + 2) & 3) * NF * PL;
-        T* const m_p1 = sm + G::OFF_M + (size_t)((q + 1) & 1) * PL;  // mu of plane p-1
-        T* const m_p2 = sm + G::OFF_M + (size_t)(q & 1) * PL;        // mu of plane p-2
+        T* const y_p = sm + G::OFF_Y + (size_t)jy * NF * PL;
+        T* const y_p1 = sm + G::OFF_Y + (size_t)((jy + 3) & 3) * NF * PL;
+        T* const y_p2 = sm + G::OFF_Y + (size_t)((jy + 2) & 3) * NF * PL;
+        T* const m_p1 = sm + G::OFF_M + (size_t)((jy + 3) & 1) * PL;  // mu of plane p-1
+        T* const m_p2 = sm + G::OFF_M + (size_t)((jy + 2) & 1) * PL;  // mu of plane p-2
         const int z = p - 2;
-        const bool do_k = z >= z0 && z < z1;
-        const bool do_mu = p - 1 >= z0 - 1 && p - 1 <= z1;
+        if constexpr (SHIFT) {
+            // planes p-2 .. p-1 (c), p-3 .. p-1 (eta) and p-3 .. p-2 (mu) move
+            // to the window indices 1..2, 0..2 and 0..1
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                w0[r][1] = w0[r][2]; w0[r][2] = w0[r][3];
+                w1[r][0] = w1[r][1]; w1[r][1] = w1[r][2]; w1[r][2] = w1[r][3];
+                wm[r][0] = wm[r][1]; wm[r][1] = wm[r][2];
+            }
+        }
 
         // the final stage's k1, k2 and low parts of this thread's tile cells at
         // plane p-2, fetched now so that they arrive while the plane is formed
         T pk1[R][2], pk2[R][2], plo[R][2];
-        if (FINAL && do_k) {
+        if (FINAL && DO_K) {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (!((tm >> r) & 1u)) continue;
@@ -258,12 +277,15 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, R, MODE != MODE_K>::NT
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            w0[r][0] = w0[r][1]; w0[r][1] = w0[r][2]; w0[r][2] = y[r][0];
-            if (NF > 1) { w1[r][0] = w1[r][1]; w1[r][1] = w1[r][2]; w1[r][2] = w1[r][3]; w1[r][3] = y[r][NF - 1]; }
+            w0[r][J] = y[r][0];
+            if (NF > 1) w1[r][J] = y[r][NF - 1];
 #pragma unroll
             for (int f = 0; f < NF; ++f) y_p[f * PL + po + r * WB] = y[r][f];
         }
-        if (__syncthreads_or(!ok)) { failed = true; break; }
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            return false;
+        }
         // the slot of plane p - RES is free (last read by step p-1): plane p + LA into it
         if (threadIdx.x == 0 && p + LA <= t_last) {
             m2::fence_proxy_async();
@@ -287,18 +309,18 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, R, MODE != MODE_K>::NT
         //      store them where nobody reads), so the rows interleave freely;
         //      with one row per thread, threads off the tile + 1 skip the phase
         //      (whole warps of the halo rows then issue nothing)
-        if (do_mu && (R > 1 || r1m)) {
+        if (DO_MU && (R > 1 || r1m)) {
             T muv[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const T cc = w0[r][1];
+                const T cc = w0[r][J1];
                 const T v2 = rmul((T)2, cc);
                 T tx, ty;
                 if (inner) {
                     const T* c = y_p1 + po + r * WB;
                     tx = second_diff(c[1], v2, c[-1]);
-                    const T cn = r + 1 < R ? w0[r + 1 < R ? r + 1 : r][1] : c[WB];
-                    const T cs = r > 0 ? w0[r > 0 ? r - 1 : r][1] : c[-WB];
+                    const T cn = r + 1 < R ? w0[r + 1 < R ? r + 1 : r][J1] : c[WB];
+                    const T cs = r > 0 ? w0[r > 0 ? r - 1 : r][J1] : c[-WB];
                     ty = second_diff(cn, v2, cs);
                 } else {
                     // the stencil centre: this cell, or the clamped cell on a zero-flux side
@@ -310,13 +332,13 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, R, MODE != MODE_K>::NT
                     tx = second_diff(c[1], v2, c[-1]);
                     ty = second_diff(c[WB], v2, c[-WB]);
                 }
-                const T tz = second_diff(w0[r][2], v2, w0[r][0]);
+                const T tz = second_diff(w0[r][J], v2, w0[r][J2]);
                 const T lap = lap_combine<T, 3>(tx, ty, tz, i2x, i2y, i2z);
-                muv[r] = pol.mu(S, cc, lap, NF > 1 ? w1[r][2] : (T)0);
+                muv[r] = pol.mu(S, cc, lap, NF > 1 ? w1[r][J1] : (T)0);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                wm[r][0] = wm[r][1]; wm[r][1] = wm[r][2]; wm[r][2] = muv[r];
+                wm[r][J1] = muv[r];
                 m_p1[po + r * WB] = muv[r];
             }
         }
@@ -324,31 +346,31 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, R, MODE != MODE_K>::NT
         // stored before the barrier above)
         // ---- the right-hand side at plane p-2 on the tile: formed for every
         //      row of the thread, stored for the tile's rows
-        if (do_k && (R > 1 || tm)) {
+        if (DO_K && (R > 1 || tm)) {
             T kv[R][2];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int o = po + r * WB;
                 const T* m = m_p2 + o;
-                const T mv2 = rmul((T)2, wm[r][1]);
+                const T mv2 = rmul((T)2, wm[r][J2]);
                 const T mtx = second_diff(m[1], mv2, m[-1]);
-                const T mn = r + 1 < R ? wm[r + 1 < R ? r + 1 : r][1] : m[WB];
-                const T ms = r > 0 ? wm[r > 0 ? r - 1 : r][1] : m[-WB];
+                const T mn = r + 1 < R ? wm[r + 1 < R ? r + 1 : r][J2] : m[WB];
+                const T ms = r > 0 ? wm[r > 0 ? r - 1 : r][J2] : m[-WB];
                 const T mty = second_diff(mn, mv2, ms);
-                const T mtz = second_diff(wm[r][2], mv2, wm[r][0]);
+                const T mtz = second_diff(wm[r][J1], mv2, wm[r][J3]);
                 const T lapmu = lap_combine<T, 3>(mtx, mty, mtz, i2x, i2y, i2z);
                 T lapy1 = (T)0;
                 if (Pol::LAP_Y1) {
                     const T* e = y_p2 + (NF - 1) * PL + o;
-                    const T ev2 = rmul((T)2, w1[r][1]);
+                    const T ev2 = rmul((T)2, w1[r][J2]);
                     const T etx = second_diff(e[1], ev2, e[-1]);
-                    const T en = r + 1 < R ? w1[r + 1 < R ? r + 1 : r][1] : e[WB];
-                    const T es = r > 0 ? w1[r > 0 ? r - 1 : r][1] : e[-WB];
+                    const T en = r + 1 < R ? w1[r + 1 < R ? r + 1 : r][J2] : e[WB];
+                    const T es = r > 0 ? w1[r > 0 ? r - 1 : r][J2] : e[-WB];
                     const T ety = second_diff(en, ev2, es);
-                    const T etz = second_diff(w1[r][2], ev2, w1[r][0]);
+                    const T etz = second_diff(w1[r][J1], ev2, w1[r][J3]);
                     lapy1 = lap_combine<T, 3>(etx, ety, etz, i2x, i2y, i2z);
                 }
-                pol.rhs(S, lapmu, w0[r][0], (T)0, NF > 1 ? w1[r][1] : (T)0, lapy1, kv[r]);
+                pol.rhs(S, lapmu, w0[r][J2], (T)0, NF > 1 ? w1[r][J2] : (T)0, lapy1, kv[r]);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -377,37 +399,70 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, R, MODE != MODE_K>::NT
                 }
             }
         }
-        if (do_k) {
-            if (FINAL) {
-                // ghost cells of the new state (the BC-mapped old state), as stage_march3d writes them
-                if (!inner) {
-                    if (x0 == 0 || x0 + TX >= n0)
-                        for (int i = threadIdx.x; i < TY * gh; i += G::NT) {
-                            const int qy = y0 + i / gh, l = 1 + i % gh;
-                            if (qy >= n1) continue;
-                            if (x0 == 0) write_ghost<T, 3>(S, NF, -l, qy, z);
-                            if (x0 + TX >= n0) write_ghost<T, 3>(S, NF, n0 - 1 + l, qy, z);
-                        }
-                    if (y0 == 0 || y0 + TY >= n1)
-                        for (int i = threadIdx.x; i < TX * gh; i += G::NT) {
-                            const int qxx = x0 + i % TX, l = 1 + i / TX;
-                            if (qxx >= n0) continue;
-                            if (y0 == 0) write_ghost<T, 3>(S, NF, qxx, -l, z);
-                            if (y0 + TY >= n1) write_ghost<T, 3>(S, NF, qxx, n1 - 1 + l, z);
-                        }
-                }
-                if (z == 0 || z == n2 - 1)
-                    for (int i = threadIdx.x; i < TX * TY * gh; i += G::NT) {
-                        const int qxx = x0 + i % TX, qy = y0 + (i / TX) % TY, l = 1 + i / (TX * TY);
-                        if (qxx >= n0 || qy >= n1) continue;
-                        if (z == 0) write_ghost<T, 3>(S, NF, qxx, qy, -l);
-                        if (z == n2 - 1) write_ghost<T, 3>(S, NF, qxx, qy, n2 - 1 + l);
-                    }
-            }
-        }
         si = si + 1 == NS ? 0 : si + 1;
         ph ^= si == 0 ? 1u : 0u;
-        yi = (yi + 1) & 3;
+        return true;
+    };
+
+    // ghost cells of the new state on planes za .. zb (the BC-mapped old state),
+    // as stage_march3d writes them; once per group of planes, outside the plane
+    // bodies, whose registers they would otherwise share
+    auto ghosts = [&](const int za, const int zb) {
+        for (int z = za; z <= zb; ++z) {
+            if (!inner) {
+                if (x0 == 0 || x0 + TX >= n0)
+                    for (int i = threadIdx.x; i < TY * gh; i += G::NT) {
+                        const int qy = y0 + i / gh, l = 1 + i % gh;
+                        if (qy >= n1) continue;
+                        if (x0 == 0) write_ghost<T, 3>(S, NF, -l, qy, z);
+                        if (x0 + TX >= n0) write_ghost<T, 3>(S, NF, n0 - 1 + l, qy, z);
+                    }
+                if (y0 == 0 || y0 + TY >= n1)
+                    for (int i = threadIdx.x; i < TX * gh; i += G::NT) {
+                        const int qxx = x0 + i % TX, l = 1 + i / TX;
+                        if (qxx >= n0) continue;
+                        if (y0 == 0) write_ghost<T, 3>(S, NF, qxx, -l, z);
+                        if (y0 + TY >= n1) write_ghost<T, 3>(S, NF, qxx, n1 - 1 + l, z);
+                    }
+            }
+            if (z == 0 || z == n2 - 1)
+                for (int i = threadIdx.x; i < TX * TY * gh; i += G::NT) {
+                    const int qxx = x0 + i % TX, qy = y0 + (i / TX) % TY, l = 1 + i / (TX * TY);
+                    if (qxx >= n0 || qy >= n1) continue;
+                    if (z == 0) write_ghost<T, 3>(S, NF, qxx, qy, -l);
+                    if (z == n2 - 1) write_ghost<T, 3>(S, NF, qxx, qy, n2 - 1 + l);
+                }
+        }
+    };
+
+    // the march: planes z0-2 and z0-1 bring inputs only, z0 and z0+1 add mu,
+    // then every plane forms mu and a right-hand side; four planes per pass so
+    // that the ring positions are compile-time (t_last >= z0 + 2 always)
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    using I2 = std::integral_constant<int, 2>;
+    using I3 = std::integral_constant<int, 3>;
+    using NO = std::false_type;
+    using YES = std::true_type;
+    if constexpr (!FINAL) {
+        if (plane(I0{}, NO{}, NO{}, t_first) && plane(I1{}, NO{}, NO{}, t_first + 1) &&
+            plane(I2{}, YES{}, NO{}, t_first + 2) && plane(I3{}, YES{}, NO{}, t_first + 3)) {
+            for (int p = t_first + 4; p <= t_last; p += 4) {
+                if (!plane(I0{}, YES{}, YES{}, p)) break;
+                if (p + 1 > t_last || !plane(I1{}, YES{}, YES{}, p + 1)) break;
+                if (p + 2 > t_last || !plane(I2{}, YES{}, YES{}, p + 2)) break;
+                if (p + 3 > t_last || !plane(I3{}, YES{}, YES{}, p + 3)) break;
+            }
+        }
+    } else {
+        using IR = std::integral_constant<int, -1>;  // rolling
+        if (plane(IR{}, NO{}, NO{}, t_first) && plane(IR{}, NO{}, NO{}, t_first + 1) &&
+            plane(IR{}, YES{}, NO{}, t_first + 2) && plane(IR{}, YES{}, NO{}, t_first + 3)) {
+            for (int p = t_first + 4; p <= t_last; ++p) {
+                if (!plane(IR{}, YES{}, YES{}, p)) break;
+                ghosts(p - 2, p - 2);
+            }
+        }
     }
 
     if (failed) {
