@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, R, MODE != MODE_K>::NT
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (!((tm >> r) & 1u)) continue;
-                const int o = po + r * WB;
+                [[maybe_unused]] const int o = po + r * WB;  // the update's slot offset
                 const int idx = L.origin + gtile + s1 * r + s2 * z;
 #pragma unroll
                 for (int f = 0; f < NF; ++f) {
