@@ -199,3 +199,30 @@ def test_streamed_3d_tile_variants_agree(cuda, prec, case):
             pa, pb = grid.phys(a), grid.phys(b)
             bad = np.argwhere(pa != pb)
             assert bad.size == 0, f"tile {tile}: {len(bad)} cells differ, first (z, y, x) {bad[:4].tolist()}"
+
+
+@pytest.mark.parametrize("prec", [px.F64, px.F32], ids=["f64", "f32"])
+def test_3d_autotune_keeps_state_and_bits(cuda, prec):
+    """The autotuner times every 3-D candidate (streamed tile variants, the
+    marching kernel, the fused two-stage launches), restores the loaded
+    state, and the form it keeps gives the marching kernel's bits."""
+    phys, n = px.PHYS_CHAC, (40, 24, 18)
+    bcs = (px.BC_NOFLUX, px.BC_NOFLUX) + (px.BC_PERIODIC,) * 4
+    g = px.make_grid(n, (1.0, 1.0, 1.0), 1, bcs)
+    grid = Grid(n=n, bc=bcs)
+    fields = _inputs(phys, n, grid, 31)
+    st = px.Stepper(phys, px.RK4, prec, PRM[phys], DT[phys], g)
+    d = [torch.from_numpy(f.copy()).cuda() for f in fields]
+    st.load(d)
+    assert st.autotune(2) > 0
+    fused, tile = st.tiles()
+    assert st.launches_per_step == (2 if fused else 4)
+    assert tile in ((0, 1) if fused else (-1, 2, 4, 5))
+    st.advance(6)
+    st.store(d)
+    torch.cuda.synchronize()
+    st.status()
+    st.close()
+    ref, _ = _run(phys, g, prec, fields, False, nsteps=6, tile=MARCH_TILE)
+    for a, b in zip([x.cpu().numpy() for x in d], ref):
+        assert np.array_equal(grid.phys(a), grid.phys(b))
