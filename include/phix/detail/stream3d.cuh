@@ -20,7 +20,11 @@
 // The z-neighbours of every stencil come from registers, so do the y-neighbours
 // of a thread's inner rows; x-neighbours (and the y-neighbours of its first and
 // last row) come from the shared planes.  The slot offsets are fixed for the
-// whole march, so a stage costs a few shared-memory accesses per cell.
+// whole march, so a stage costs a few shared-memory accesses per cell.  One CTA
+// barrier per plane (after the stage-state store) orders every shared slot's
+// reuse.  The k stages march four planes per pass, so that the ring positions
+// of the windows and slots are compile-time; the update, whose extra operands
+// leave no registers for that, rolls one plane at a time.
 //
 // Boundaries: z periodic (the plane index wraps before the copy); x and y
 // periodic or zero-flux.  Input cells outside the grid are replaced after the
