@@ -187,7 +187,7 @@ TRAFFIC = {
     ("ch2d_ms", "f64", "step_pair_ms"): 8.45e6,  # CH 1024^2 multi-step Euler
     # CH+AC 256^3 RK4, one launch per stage: mean over the four launches of a time step
     ("chac3d", "f32", "stage_stream3d"): 510.0e6,
-    ("chac3d", "f64", "stage_stream3d"): 883.0e6,
+    ("chac3d", "f64", "stage_stream3d"): 914.0e6,
 }
 
 # Lane operations (fma = 2) of one RK4 cell-update in step2d_pair.cuh, on the

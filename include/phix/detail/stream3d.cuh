@@ -76,7 +76,8 @@ struct Stream3 {
     static constexpr int RES = FINAL ? 3 : 1;
     // one row per thread leaves room for a deeper ring; R rows per thread hold
     // R times the cells of a thread in every slot
-    static constexpr int LA = R > 1 ? 2 : FINAL ? (sizeof(T) == 4 ? 3 : 2) : (sizeof(T) == 4 ? 6 : 4);
+    // (FP64 k stages on tiles of fewer than 8 rows: 2, so that three CTAs fit)
+    static constexpr int LA = R > 1 ? 2 : FINAL ? (sizeof(T) == 4 ? 3 : 2) : (sizeof(T) == 4 ? 6 : TY < 8 ? 2 : 4);
     static constexpr int NS = RES + LA;
     // shared planes of y (p-3 .. p) and mu (p-2, p-1).  One CTA barrier per
     // plane (after the y store): every slot is rewritten only after the barrier
@@ -93,8 +94,9 @@ struct Stream3 {
     static constexpr size_t smem_bytes() { return 128 + BAR_OFF + NS * 8; }
     static constexpr uint32_t BOX_BYTES = (uint32_t)(WB * HB * sizeof(T));
     // CTAs per SM the registers are budgeted for: as many as the shared memory
-    // holds with one row per thread (FP32 k stages: 3, else 2)
-    static constexpr int MIN_CTAS = R == 1 ? (sizeof(T) == 4 && !FINAL ? 3 : 2) : 1;
+    // holds with one row per thread (FP32 k stages and FP64 ones on tiles of
+    // fewer than 8 rows: 3, else 2)
+    static constexpr int MIN_CTAS = R == 1 ? ((sizeof(T) == 4 || TY < 8) && !FINAL ? 3 : 2) : 1;
     static_assert(Pol::MU && H == 2, "the streaming 3-D stage is built for the chemical-potential physics");
     static_assert(NY % R == 0 && R >= 1 && R <= 8, "the rows of the tile + 2 split into whole groups of R");
     static_assert(WB <= 256 && HB <= 256 && NT <= 1024, "tile too large");

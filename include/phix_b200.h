@@ -205,8 +205,8 @@ int phix_stepper_depth(const phix_stepper_t* h);
  * per stage, -1 (and 0, 1) streams CH / CH+AC grids (z periodic; x, y
  * periodic or zero-flux) through the TMA-staged kernel on its default tile,
  * 3..5 pick that kernel's tile variants (FP32: 32x8 with one row per thread,
- * 32x16 with four, 32x8 with two; FP64: 32x8 with one, two, four rows per
- * thread), and 2 selects the marching kernel without TMA; on the fused
+ * 32x16 with four, 32x6 with one; FP64: 32x6 with one, 32x8 with two and
+ * with one), and 2 selects the marching kernel without TMA; on the fused
  * two-stage RK4 path 0 (the default) or 1 pick two tile variants (the second
  * puts the stages-3-4 launch on 32x8 tiles).  -1 picks by grid (see
  * phix_stepper_autotune for a measured choice).  All give the same bits.

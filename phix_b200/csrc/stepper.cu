@@ -750,15 +750,16 @@ int m2_dispatch(int phys, bool prepare, March2Args<T>* a, cudaStream_t s, bool s
 
 // ---- one stage of the mu physics streamed through z (stream3d.cuh) --------
 // tile variants per precision: TX x TY tile, R rows of a column per thread,
-// (TX + 4) x (TY + 4) / R threads
+// (TX + 4) x (TY + 4) / R threads; variant 0 is the default (measured fastest
+// at 256^3: FP32 32x8, FP64 32x6, whose k stages fit three CTAs per SM)
 constexpr int kNumS3Variants = 3;
 template <typename T, int V> struct S3Cfg;
 template <> struct S3Cfg<float, 0> { static constexpr int TX = 32, TY = 8, R = 1; };
 template <> struct S3Cfg<float, 1> { static constexpr int TX = 32, TY = 16, R = 4; };
-template <> struct S3Cfg<float, 2> { static constexpr int TX = 32, TY = 8, R = 2; };
-template <> struct S3Cfg<double, 0> { static constexpr int TX = 32, TY = 8, R = 1; };
+template <> struct S3Cfg<float, 2> { static constexpr int TX = 32, TY = 6, R = 1; };
+template <> struct S3Cfg<double, 0> { static constexpr int TX = 32, TY = 6, R = 1; };
 template <> struct S3Cfg<double, 1> { static constexpr int TX = 32, TY = 8, R = 2; };
-template <> struct S3Cfg<double, 2> { static constexpr int TX = 32, TY = 8, R = 4; };
+template <> struct S3Cfg<double, 2> { static constexpr int TX = 32, TY = 8, R = 1; };
 
 template <typename T, class Pol, int MODE, int V>
 int s3_kernel(bool prepare, Stream3Args<T>* a, cudaStream_t s) {
