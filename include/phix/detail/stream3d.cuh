@@ -127,8 +127,23 @@ __global__ void __launch_bounds__(Stream3<T, Pol, TX, TY, R, MODE != MODE_K>::NT
     // the tile + 2 lies inside the grid: no BC mapping, no clamped mu
     const bool inner = x0 - H >= 0 && x0 + TX + H <= n0 && y0 - H >= 0 && y0 + TY + H <= n1;
 
-    // this thread's column and rows
-    const int cx = threadIdx.x % NX, grp = threadIdx.x / NX;
+    // this thread's column and rows: warps take 32 columns of one row group
+    // (one bank each in a shared plane, no conflicts), the last threads the
+    // NX - 32 columns left over in every group
+    int cx, grp;
+    if constexpr (NX > 32) {
+        constexpr int MAIN = 32 * G::NG;
+        if ((int)threadIdx.x < MAIN) {
+            cx = threadIdx.x % 32;
+            grp = threadIdx.x / 32;
+        } else {
+            cx = 32 + ((int)threadIdx.x - MAIN) % (NX - 32);
+            grp = ((int)threadIdx.x - MAIN) / (NX - 32);
+        }
+    } else {
+        cx = threadIdx.x % NX;
+        grp = threadIdx.x / NX;
+    }
     const int lx = cx - H, px = x0 + lx;
     const int ly0 = grp * R - H, py0 = y0 + ly0;  // its first row
     const int po = (cx + sh) + grp * R * WB;      // slot offset of its first row
